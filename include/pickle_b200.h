@@ -1,0 +1,137 @@
+/*
+ * pickle_b200 — C ABI of the B200 HNSW index (query and insert path).
+ *
+ * The reference (juelinl/pickle) exposes its HNSW index only as a header-only
+ * C++ template class, pickle::v2::HNSWGraph (include/hnsw.hpp:23-220).  This
+ * library implements the same index on the GPU and exposes it through plain C
+ * entry points, so that any host language can bind it (ctypes, cgo, JNI, a C++
+ * header such as include/pickle_b200/hnsw.hpp).  Each entry point below names
+ * the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every call returns an int status: PK_OK (0) or a negative PK_ERR_* code.
+ *    pk_last_error() gives a message for the calling thread's last failure.
+ *    The reference has no error codes (it asserts or calls exit(-1),
+ *    include/marco.hpp:20-68); here nothing aborts the process.
+ *  - Enumerations keep the reference's numeric values: metric is DistFunc
+ *    (1 = L2, 2 = IP; include/common.hpp:28-33), dtype is DataType
+ *    (0 = uint8, 1 = int8, 2 = float32, 3 = float16; include/common.hpp:21-26).
+ *  - Distances are returned as the reference returns them: squared L2, or the
+ *    negated inner product (include/distance/avx512.hpp:233-243), ascending.
+ *  - Vectors are row-major, dim elements per row, element type = dtype.
+ *  - The index owns its device memory; caller buffers are only borrowed for
+ *    the duration of a call (host variants) or until the given stream reaches
+ *    the end of the call's work (device variants).
+ *  - A handle may be used by one thread at a time.
+ */
+#ifndef PICKLE_B200_H
+#define PICKLE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PK_OK 0
+#define PK_ERR_ARG (-1)         /* bad argument */
+#define PK_ERR_OOM (-2)         /* host or device allocation failed */
+#define PK_ERR_IO (-3)          /* file could not be opened / read / written */
+#define PK_ERR_FORMAT (-4)      /* not a v2 graph file, bad header, bad checksum */
+#define PK_ERR_CUDA (-5)        /* a CUDA call failed */
+#define PK_ERR_STATE (-6)       /* call not valid in the index's state */
+#define PK_ERR_TIMEOUT (-7)     /* a device-side wait ran out of its budget */
+#define PK_ERR_OVERFLOW (-8)    /* a search outgrew its scratch even after retry */
+#define PK_ERR_NO_DEVICE (-9)   /* no CUDA device */
+#define PK_ERR_CAPACITY (-10)   /* external id beyond the reserved capacity */
+
+#define PK_METRIC_L2 1
+#define PK_METRIC_IP 2
+
+#define PK_DTYPE_U8 0
+#define PK_DTYPE_I8 1
+#define PK_DTYPE_F32 2
+#define PK_DTYPE_F16 3
+
+typedef struct pk_index pk_index;
+
+/* Message for the calling thread's most recent failed call ("" if none). */
+const char *pk_last_error(void);
+
+/* Library version: major * 10000 + minor * 100 + patch. */
+int pk_version(void);
+
+/* Replaces HNSWGraph(max_degree, build_ef, DistFunc) / HNSWGraph::Init
+ * (include/hnsw.hpp:27-36).  M is the upper-layer degree cap; layer 0 holds
+ * 2*M slots per node (include/hnsw.hpp:235).  The index is bound to the
+ * current CUDA device. */
+int pk_index_create(pk_index **out, int metric, int dtype, int64_t dim, int64_t M, int64_t ef_construction);
+
+/* Frees the handle and all its device memory.  NULL is accepted. */
+int pk_index_destroy(pk_index *h);
+
+/* Sets the seed of the per-node level draw (default 0).  The reference draws
+ * levels from std::random_device (include/util.hpp:172-198); here level(ext_id)
+ * is a pure function of (seed, ext_id) with the same distribution, so builds
+ * are reproducible.  Must be called before the first insertion. */
+int pk_index_set_seed(pk_index *h, uint64_t seed);
+
+/* Sets per-node levels explicitly for external ids [0, n) (one byte each).
+ * Replaces the level draw of InitBuffer (include/hnsw.hpp:222-245); used to
+ * reproduce a given build.  Must be called before the first insertion. */
+int pk_index_set_levels(pk_index *h, const uint8_t *levels, int64_t n);
+
+/* Replaces HNSWGraph::Build (include/hnsw.hpp:497-507): inserts the rows of
+ * data (n rows, host memory, indexed by external id) in the order given by
+ * ext_ids (NULL = 0, 1, ..., n-1).  External ids must lie in [0, n).
+ * Insertion runs on the GPU in batches of at most max_batch nodes
+ * (0 = automatic); max_batch = 1 reproduces a one-thread build of the
+ * reference algorithm exactly (with adjacency lists bounded by their caps). */
+int pk_index_build(pk_index *h, const void *data, int64_t n, const int32_t *ext_ids, int32_t max_batch);
+
+/* Replaces HNSWGraph::Insert (include/hnsw.hpp:247-302) for a batch: inserts
+ * n new rows (host memory, row i has external id ext_ids[i]) into an existing
+ * index.  External ids must be unused; the index grows as needed. */
+int pk_index_add(pk_index *h, const void *rows, int64_t n, const int32_t *ext_ids, int32_t max_batch);
+
+/* Replaces HNSWGraph::AnnSearch(top_k, search_ef, NDArray) (include/hnsw.hpp:528-541).
+ * Host buffers: queries nq*dim, out_ids / out_dists nq*k.  Rows with fewer than
+ * k results are padded with id -1 and distance FLT_MAX.  Synchronous. */
+int pk_index_search(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
+                    float *out_dists);
+
+/* Device-resident batch search, asynchronous on `stream` (a cudaStream_t,
+ * NULL = legacy default stream).  All pointers are device pointers.
+ *  k_per_query / ef_per_query: nq values each, or NULL to use k / ef for all.
+ *  Results for query i go to out_ids/out_dists + i*out_stride (out_stride >=
+ *  the largest k).  counters (nullable) receives nq*6 int32 values per query:
+ *  hops, distance evaluations and neighbours scanned on the upper layers,
+ *  then the same three on layer 0 (the Profiler quantities of
+ *  include/profiler.hpp:13-69).
+ *  Results are identical to pk_index_search's.  The call may synchronise
+ *  `stream` once to retry the rare queries that outgrow their scratch. */
+int pk_index_search_device(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                           const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride,
+                           int32_t *out_ids, float *out_dists, int32_t *counters, void *stream);
+
+/* Replaces the Serializer::to_disk / from_disk pair that the reference names
+ * for persistence (include/serializer.hpp:21-25) but only implements for its
+ * retired v0 layer.  Writes / reads the v2 graph file (format described in
+ * DESIGN.md and pickle_b200/csrc/pk_format.cpp). */
+int pk_index_save(const pk_index *h, const char *path);
+int pk_index_load(pk_index **out, const char *path);
+
+/* out[0..11] = n (nodes), num_layers, enter_level, capacity, dim, M,
+ * ef_construction, metric, dtype, device bytes held, layer-0 cap, entry id. */
+int pk_index_info(const pk_index *h, int64_t *out);
+
+/* Copies one layer's structure to host buffers (each may be NULL):
+ * ext[n], degree[n], heuristic[n], has_vector[n], adj[layer_capacity*cap],
+ * dist[layer_capacity*cap].  *n, *layer_capacity and *cap are always written. */
+int pk_index_layer(const pk_index *h, int level, int64_t *n, int64_t *layer_capacity, int64_t *cap, int32_t *ext,
+                   int16_t *degree, int16_t *heuristic, uint8_t *has_vector, int32_t *adj, float *dist);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,210 @@
+"""pickle_b200: a B200 HNSW index (query and insert path) behind a C ABI.
+
+The native library ``libpickle_b200.so`` (built by ``python -m pickle_b200.build``)
+holds the whole index on the GPU and exports the entry points declared in
+``include/pickle_b200.h``.  This module binds them with ctypes and offers
+``HNSWIndex``, whose method names follow the reference's (broken) Python
+binding (pybind/hnsw.cpp:116-128: build / search / save / load) and whose
+semantics follow pickle::v2::HNSWGraph (include/hnsw.hpp:23-220).
+
+There is no CPU implementation here: if the library is missing or no GPU is
+present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["HNSWIndex", "PickleError", "lib", "DTYPES", "METRICS", "LIB_PATH"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpickle_b200.so")
+
+# DataType and DistFunc values of the reference (include/common.hpp:21-33)
+DTYPES = {np.dtype(np.uint8): 0, np.dtype(np.int8): 1, np.dtype(np.float32): 2, np.dtype(np.float16): 3}
+NP_OF = {v: k for k, v in DTYPES.items()}
+METRICS = {"l2": 1, "ip": 2}
+
+ERRORS = {
+    -1: "bad argument", -2: "out of memory", -3: "I/O error", -4: "bad graph file", -5: "CUDA error",
+    -6: "invalid state", -7: "device wait timed out", -8: "scratch overflow", -9: "no CUDA device",
+    -10: "capacity exceeded",
+}
+
+
+class PickleError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m pickle_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I64, I32, VP = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p
+        PP = ctypes.POINTER(ctypes.c_void_p)
+        L.pk_last_error.restype = ctypes.c_char_p
+        L.pk_version.restype = ctypes.c_int
+        L.pk_index_create.argtypes = [PP, ctypes.c_int, ctypes.c_int, I64, I64, I64]
+        L.pk_index_destroy.argtypes = [P]
+        L.pk_index_set_seed.argtypes = [P, ctypes.c_uint64]
+        L.pk_index_set_levels.argtypes = [P, VP, I64]
+        L.pk_index_build.argtypes = [P, VP, I64, VP, I32]
+        L.pk_index_add.argtypes = [P, VP, I64, VP, I32]
+        L.pk_index_search.argtypes = [P, VP, I64, I32, I32, VP, VP]
+        L.pk_index_search_device.argtypes = [P, VP, I64, I32, I32, VP, VP, I32, VP, VP, VP, VP]
+        L.pk_index_save.argtypes = [P, ctypes.c_char_p]
+        L.pk_index_load.argtypes = [PP, ctypes.c_char_p]
+        L.pk_index_info.argtypes = [P, VP]
+        L.pk_index_layer.argtypes = [P, ctypes.c_int] + [VP] * 3 + [VP] * 6
+        for name in ["pk_index_create", "pk_index_destroy", "pk_index_set_seed", "pk_index_set_levels",
+                     "pk_index_build", "pk_index_add", "pk_index_search", "pk_index_search_device",
+                     "pk_index_save", "pk_index_load", "pk_index_info", "pk_index_layer"]:
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise PickleError(rc, lib().pk_last_error().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _dev_ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class HNSWIndex:
+    """An HNSW index resident in GPU memory.
+
+    HNSWIndex(dim, dtype, metric="l2", M=32, ef_construction=100) mirrors
+    HNSWGraph(max_degree, build_ef, DistFunc) (include/hnsw.hpp:27-36).
+    """
+
+    def __init__(self, dim: int = 0, dtype=np.float32, metric: str = "l2", M: int = 32,
+                 ef_construction: int = 100, _handle=None):
+        self._h = None
+        if _handle is not None:
+            self._h = _handle
+        else:
+            h = ctypes.c_void_p()
+            _check(lib().pk_index_create(ctypes.byref(h), METRICS[metric], DTYPES[np.dtype(dtype)], dim, M,
+                                         ef_construction))
+            self._h = h
+        info = self.info()
+        self.dim = info["dim"]
+        self.dtype = NP_OF[info["dtype"]]
+        self.metric = {1: "l2", 2: "ip"}[info["metric"]]
+        self.M = info["M"]
+        self.ef_construction = info["ef_construction"]
+
+    def __del__(self):
+        self.close()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().pk_index_destroy(self._h)
+            self._h = None
+
+    # ---- construction -------------------------------------------------
+    def set_seed(self, seed: int) -> None:
+        _check(lib().pk_index_set_seed(self._h, seed))
+
+    def set_levels(self, levels: np.ndarray) -> None:
+        lv = np.ascontiguousarray(levels, dtype=np.uint8)
+        _check(lib().pk_index_set_levels(self._h, _ptr(lv), len(lv)))
+
+    def build(self, data: np.ndarray, ext_ids: np.ndarray | None = None, max_batch: int = 0) -> None:
+        """HNSWGraph::Build: insert data[ext_ids[i]] with id ext_ids[i], i = 0..n-1."""
+        data = self._rows(data)
+        ids = None if ext_ids is None else np.ascontiguousarray(ext_ids, dtype=np.int32)
+        _check(lib().pk_index_build(self._h, _ptr(data), data.shape[0], _ptr(ids) if ids is not None else None,
+                                    max_batch))
+
+    def add(self, rows: np.ndarray, ext_ids: np.ndarray, max_batch: int = 0) -> None:
+        """HNSWGraph::Insert for a batch of new rows."""
+        rows = self._rows(rows)
+        ids = np.ascontiguousarray(ext_ids, dtype=np.int32)
+        if len(ids) != rows.shape[0]:
+            raise ValueError("one external id per row")
+        _check(lib().pk_index_add(self._h, _ptr(rows), rows.shape[0], _ptr(ids), max_batch))
+
+    # ---- queries --------------------------------------------------------
+    def search(self, queries: np.ndarray, k: int, ef: int):
+        """HNSWGraph::AnnSearch(k, ef, queries): (ids, dists), each nq x k, ascending."""
+        q = self._rows(queries)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.int32)
+        dists = np.empty((nq, k), np.float32)
+        _check(lib().pk_index_search(self._h, _ptr(q), nq, k, ef, _ptr(ids), _ptr(dists)))
+        return ids, dists
+
+    def search_device(self, queries, k: int, ef: int, out_ids, out_dists, k_per_query=None, ef_per_query=None,
+                      counters=None, stream=None) -> None:
+        """Device-resident search on torch CUDA tensors (asynchronous on `stream`).
+
+        queries: (nq, dim) contiguous; out_ids int32 / out_dists float32: (nq, stride);
+        k_per_query / ef_per_query: optional int32 (nq,); counters: optional int32 (nq, 6).
+        """
+        nq = queries.shape[0]
+        stride = out_ids.shape[1]
+        s = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _check(lib().pk_index_search_device(self._h, _dev_ptr(queries), nq, k, ef, _dev_ptr(k_per_query),
+                                            _dev_ptr(ef_per_query), stride, _dev_ptr(out_ids), _dev_ptr(out_dists),
+                                            _dev_ptr(counters), s))
+
+    # ---- persistence ----------------------------------------------------
+    def save(self, path: str) -> None:
+        _check(lib().pk_index_save(self._h, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, path: str) -> "HNSWIndex":
+        h = ctypes.c_void_p()
+        _check(lib().pk_index_load(ctypes.byref(h), os.fsencode(path)))
+        return cls(_handle=h)
+
+    # ---- introspection --------------------------------------------------
+    def info(self) -> dict:
+        out = np.zeros(12, np.int64)
+        _check(lib().pk_index_info(self._h, _ptr(out)))
+        keys = ["n", "num_layers", "enter_level", "capacity", "dim", "M", "ef_construction", "metric", "dtype",
+                "device_bytes", "cap0", "entry"]
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def layer(self, level: int) -> dict:
+        n, lcap, cap = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().pk_index_layer(self._h, level, ctypes.byref(n), ctypes.byref(lcap), ctypes.byref(cap),
+                                    None, None, None, None, None, None))
+        n, lcap, cap = n.value, lcap.value, cap.value
+        ext = np.empty(n, np.int32)
+        deg = np.empty(n, np.int16)
+        heu = np.empty(n, np.int16)
+        hv = np.empty(n, np.uint8)
+        adj = np.empty(lcap * cap, np.int32)
+        dist = np.empty(lcap * cap, np.float32)
+        _check(lib().pk_index_layer(self._h, level, ctypes.byref(ctypes.c_int64()), ctypes.byref(ctypes.c_int64()),
+                                    ctypes.byref(ctypes.c_int64()), _ptr(ext), _ptr(deg), _ptr(heu), _ptr(hv),
+                                    _ptr(adj), _ptr(dist)))
+        return {"n": n, "layer_capacity": lcap, "cap": cap, "ext": ext, "degree": deg, "heuristic": heu,
+                "has_vector": hv, "adj": adj, "dist": dist}
+
+    def _rows(self, a: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(a)
+        if a.ndim != 2 or a.shape[1] != self.dim:
+            raise ValueError(f"expected (n, {self.dim}) rows, got {a.shape}")
+        if a.dtype != self.dtype:
+            raise TypeError(f"expected {self.dtype}, got {a.dtype}")
+        return a

@@ -1,0 +1,1193 @@
+// Host side of libpickle_b200.so: the index handle, its device memory, the
+// batched build, search dispatch and the C ABI of include/pickle_b200.h.
+//
+// Device layout (one index):
+//   vec0      layer-0 vectors, one row per layer-0 internal id (= insertion
+//             order), rows padded with zeros to a multiple of 16 bytes;
+//   per layer adj / dist (fixed stride cap, as the reference's
+//             include/hnsw_layer.hpp:76-78), deg, heu, ext, and for upper
+//             layers vrow (the vec0 row holding that layer's copy of the
+//             vector, -1 = the zero row) and down (the node's id one layer
+//             down, replacing the reference's ext2in lookups);
+//   a DevGraph block holding all of the above, read by the kernels.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <new>
+#include <stdexcept>
+#include <vector>
+
+#include "pk_build.h"
+#include "pk_format.h"
+#include "pk_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define PK_CUDA(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            return fail(e_ == cudaErrorMemoryAllocation ? PK_ERR_OOM : PK_ERR_CUDA,                \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+        }                                                                                          \
+    } while (0)
+
+#define PK_TRY(call)               \
+    do {                           \
+        int rc_ = (call);          \
+        if (rc_ != PK_OK) return rc_; \
+    } while (0)
+
+__global__ void fill_i32_kernel(int32_t *p, int64_t n, int32_t v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void fill_f32_kernel(float *p, int64_t n, float v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+cudaError_t fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    fill_i32_kernel<<<grid, 256, 0, s>>>(p, n, v);
+    return cudaGetLastError();
+}
+cudaError_t fill_f32(float *p, int64_t n, float v, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    fill_f32_kernel<<<grid, 256, 0, s>>>(p, n, v);
+    return cudaGetLastError();
+}
+
+int64_t pow2ceil(int64_t x) {
+    int64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// splitmix64: the per-node random stream of the level draw.
+inline uint64_t splitmix64(uint64_t &s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// Scratch of one kind of search launch (queries, or insertion searches).
+struct SearchScratch {
+    int64_t warps = 0;
+    int64_t slots = 0;      // visited-table slots per warp
+    unsigned long long *vis = nullptr;
+    uint32_t *epochs = nullptr;
+    void *cand_tail = nullptr;
+    int32_t *work = nullptr;
+};
+
+}  // namespace
+
+struct pk_index {
+    int device = 0;
+    int num_sms = 0;
+    int metric = 0, dtype = 0;
+    int64_t dim = 0, M = 0, efc = 0, esz = 0, row_bytes = 0;
+    pk::LaneCfg lc{};
+    uint64_t seed = 0;
+    std::vector<uint8_t> level_override;
+    bool touched = false;   // an insertion happened (seed / levels are frozen)
+    cudaStream_t stream = nullptr;
+
+    // graph
+    pk::DevGraph hg{};             // host copy holding device pointers
+    pk::DevGraph *dg = nullptr;    // device copy
+    int64_t alloc_rows[pk::kMaxLayers] = {};
+    int num_layers = 0;
+    int64_t vec_rows = 0;          // rows allocated in vec0
+    int64_t capacity = 0;          // external ids in [0, capacity)
+    std::vector<int32_t> ext_in0;  // external id -> layer-0 id (-1 absent)
+    std::vector<uint8_t> ext_level;
+    uint8_t *zero_row = nullptr;
+
+    // scratch
+    SearchScratch qs, bs;
+    uint8_t *d_qstage = nullptr;
+    int64_t qstage_rows = 0;
+    int32_t *d_ids = nullptr;
+    float *d_dists = nullptr;
+    int64_t ids_n = 0, dists_n = 0;
+    uint8_t *d_status = nullptr;
+    int64_t status_n = 0;
+    int32_t *d_qlist = nullptr;
+    int64_t qlist_n = 0;
+
+    size_t dev_bytes = 0;
+
+    int64_t n0() const { return hg.L[0].n; }
+};
+
+namespace {
+
+int dalloc(pk_index *h, void **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PK_ERR_OOM, "cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+    h->dev_bytes += bytes;
+    return PK_OK;
+}
+
+void dfree(pk_index *h, void *p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    h->dev_bytes -= std::min(h->dev_bytes, bytes == 0 ? (size_t)16 : bytes);
+}
+
+int push_graph(pk_index *h) {
+    PK_CUDA(cudaMemcpy(h->dg, &h->hg, sizeof(pk::DevGraph), cudaMemcpyHostToDevice));
+    return PK_OK;
+}
+
+// Make layer l hold at least rows node slots (plus a spare tail row).
+int ensure_layer(pk_index *h, int l, int64_t rows, int64_t cap) {
+    pk::DevLayer &L = h->hg.L[l];
+    if (l >= h->num_layers) {
+        L = pk::DevLayer{};
+        L.cap = cap;
+        h->alloc_rows[l] = 0;
+        h->num_layers = l + 1;
+        h->hg.num_layers = h->num_layers;
+    }
+    const int64_t want = rows + 1;
+    if (h->alloc_rows[l] >= want) {
+        L.lcap = std::max(L.lcap, rows);
+        return PK_OK;
+    }
+    int64_t nr = std::max<int64_t>(want, h->alloc_rows[l] + h->alloc_rows[l] / 2);
+    nr = std::max<int64_t>(nr, 16);
+    const int64_t old = h->alloc_rows[l];
+    const int64_t c = L.cap;
+    pk::DevLayer N = L;
+    PK_TRY(dalloc(h, (void **)&N.adj, sizeof(int32_t) * nr * c));
+    PK_TRY(dalloc(h, (void **)&N.dist, sizeof(float) * nr * c));
+    PK_TRY(dalloc(h, (void **)&N.deg, sizeof(int32_t) * nr));
+    PK_TRY(dalloc(h, (void **)&N.heu, sizeof(int32_t) * nr));
+    PK_TRY(dalloc(h, (void **)&N.ext, sizeof(int32_t) * nr));
+    PK_TRY(dalloc(h, (void **)&N.vrow, sizeof(int32_t) * nr));
+    PK_TRY(dalloc(h, (void **)&N.down, sizeof(int32_t) * nr));
+    cudaStream_t s = h->stream;
+    PK_CUDA(fill_i32(N.adj, nr * c, -1, s));
+    PK_CUDA(fill_f32(N.dist, nr * c, FLT_MAX, s));
+    PK_CUDA(cudaMemsetAsync(N.deg, 0, sizeof(int32_t) * nr, s));
+    PK_CUDA(cudaMemsetAsync(N.heu, 0, sizeof(int32_t) * nr, s));
+    PK_CUDA(fill_i32(N.ext, nr, -1, s));
+    PK_CUDA(fill_i32(N.vrow, nr, -1, s));
+    PK_CUDA(fill_i32(N.down, nr, -1, s));
+    if (old > 0) {
+        PK_CUDA(cudaMemcpyAsync(N.adj, L.adj, sizeof(int32_t) * old * c, cudaMemcpyDeviceToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(N.dist, L.dist, sizeof(float) * old * c, cudaMemcpyDeviceToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(N.deg, L.deg, sizeof(int32_t) * old, cudaMemcpyDeviceToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(N.heu, L.heu, sizeof(int32_t) * old, cudaMemcpyDeviceToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(N.ext, L.ext, sizeof(int32_t) * old, cudaMemcpyDeviceToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(N.vrow, L.vrow, sizeof(int32_t) * old, cudaMemcpyDeviceToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(N.down, L.down, sizeof(int32_t) * old, cudaMemcpyDeviceToDevice, s));
+        PK_CUDA(cudaStreamSynchronize(s));
+        dfree(h, L.adj, sizeof(int32_t) * old * c);
+        dfree(h, L.dist, sizeof(float) * old * c);
+        dfree(h, L.deg, sizeof(int32_t) * old);
+        dfree(h, L.heu, sizeof(int32_t) * old);
+        dfree(h, L.ext, sizeof(int32_t) * old);
+        dfree(h, L.vrow, sizeof(int32_t) * old);
+        dfree(h, L.down, sizeof(int32_t) * old);
+    }
+    N.lcap = std::max(L.lcap, rows);
+    L = N;
+    h->alloc_rows[l] = nr;
+    return PK_OK;
+}
+
+int ensure_vec(pk_index *h, int64_t rows) {
+    if (h->vec_rows >= rows) return PK_OK;
+    int64_t nr = std::max<int64_t>(rows, h->vec_rows + h->vec_rows / 2);
+    nr = std::max<int64_t>(nr, 16);
+    uint8_t *nv = nullptr;
+    PK_TRY(dalloc(h, (void **)&nv, (size_t)(nr * h->row_bytes)));
+    PK_CUDA(cudaMemsetAsync(nv, 0, (size_t)(nr * h->row_bytes), h->stream));
+    if (h->vec_rows > 0) {
+        PK_CUDA(cudaMemcpyAsync(nv, h->hg.vec0, (size_t)(h->vec_rows * h->row_bytes), cudaMemcpyDeviceToDevice,
+                                h->stream));
+        PK_CUDA(cudaStreamSynchronize(h->stream));
+        dfree(h, (void *)h->hg.vec0, (size_t)(h->vec_rows * h->row_bytes));
+    }
+    h->hg.vec0 = nv;
+    h->vec_rows = nr;
+    return PK_OK;
+}
+
+void free_scratch(pk_index *h, SearchScratch &s) {
+    dfree(h, s.vis, sizeof(unsigned long long) * s.warps * s.slots);
+    dfree(h, s.cand_tail, 8 * (size_t)s.warps * (size_t)s.slots);
+    dfree(h, s.epochs, sizeof(uint32_t) * s.warps);
+    dfree(h, s.work, sizeof(int32_t) * 4);
+    s = SearchScratch{};
+}
+
+int ensure_scratch(pk_index *h, SearchScratch &s, int64_t warps, int64_t slots) {
+    if (s.warps >= warps && s.slots == slots && s.vis) return PK_OK;
+    const int64_t w = std::max(warps, s.slots == slots ? s.warps : (int64_t)0);
+    if (s.vis) {
+        PK_CUDA(cudaStreamSynchronize(h->stream));
+        free_scratch(h, s);
+    }
+    PK_TRY(dalloc(h, (void **)&s.vis, sizeof(unsigned long long) * w * slots));
+    PK_TRY(dalloc(h, &s.cand_tail, 8 * (size_t)w * (size_t)slots));
+    PK_TRY(dalloc(h, (void **)&s.epochs, sizeof(uint32_t) * w));
+    PK_TRY(dalloc(h, (void **)&s.work, sizeof(int32_t) * 4));
+    PK_CUDA(cudaMemsetAsync(s.vis, 0, sizeof(unsigned long long) * w * slots, h->stream));
+    PK_CUDA(cudaMemsetAsync(s.epochs, 0, sizeof(uint32_t) * w, h->stream));
+    s.warps = w;
+    s.slots = slots;
+    return PK_OK;
+}
+
+template <class T>
+int ensure_buf(pk_index *h, T **p, int64_t &have, int64_t need) {
+    if (have >= need && *p) return PK_OK;
+    if (*p) {
+        PK_CUDA(cudaStreamSynchronize(h->stream));
+        dfree(h, *p, sizeof(T) * have);
+        *p = nullptr;
+    }
+    int64_t n = std::max<int64_t>(need, have + have / 2);
+    PK_TRY(dalloc(h, (void **)p, sizeof(T) * n));
+    have = n;
+    return PK_OK;
+}
+
+// ---------------------------------------------------------------- levels ----
+
+// get_cumulative_probability (include/util.hpp:13-25).
+std::vector<double> cumulative_probability(int64_t M) {
+    std::vector<double> ret;
+    const double r = 1.0 / std::log((double)M);
+    double c = 0.0;
+    for (;;) {
+        const double delta = std::exp(-1.0 * (double)ret.size() / r) * (1 - std::exp(-1.0 / r));
+        if (delta < 1e-9) break;
+        c += delta;
+        ret.push_back(c);
+    }
+    return ret;
+}
+
+// The level of one node: a fresh uniform draw per level, compared with the
+// cumulative probability (the scheme of get_random_levels,
+// include/util.hpp:172-198), from a stream keyed by (seed, external id).
+int draw_level(const std::vector<double> &cp, uint64_t seed, int32_t ext) {
+    uint64_t s = seed ^ (0xD1B54A32D192ED03ULL * (uint64_t)(uint32_t)ext + 0x8CB92BA72F3D8DD7ULL);
+    for (size_t l = 0; l < cp.size(); l++) {
+        const double u = (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0);
+        if (u < cp[l]) return (int)l;
+    }
+    return (int)cp.size() - 1;
+}
+
+// ---------------------------------------------------------------- search ----
+
+int run_search(pk_index *h, const uint8_t *d_q, int64_t nq, int32_t k, int32_t ef, const int32_t *k_arr,
+               const int32_t *ef_arr, int32_t stride, int32_t *ids, float *dists, int32_t *counters, cudaStream_t s) {
+    if (nq == 0) return PK_OK;
+    const int ef_max = std::max(ef, 1);
+    const int wcap = ef_max + 2;
+    int wpb = 4;
+    size_t smem = (size_t)wpb * pk::search_smem_per_warp(wcap);
+    while (wpb > 1 && smem > 200 * 1024) {
+        wpb /= 2;
+        smem = (size_t)wpb * pk::search_smem_per_warp(wcap);
+    }
+    if (smem > 220 * 1024) return fail(PK_ERR_ARG, "ef too large for shared memory: " + std::to_string(ef));
+    const int nb = pk::search_blocks_per_sm(h->dtype, h->lc, wpb, smem);
+    if (nb <= 0) return fail(PK_ERR_CUDA, "search kernel cannot be resident");
+    const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + wpb - 1) / wpb);
+    PK_TRY(ensure_buf(h, &h->d_status, h->status_n, nq));
+
+    int64_t slots = pow2ceil(std::max<int64_t>(2048, 32LL * ef_max + 2048));
+    const int32_t *qlist = nullptr;
+    int64_t todo = nq;
+    for (int attempt = 0; attempt < 4; attempt++) {
+        PK_TRY(ensure_scratch(h, h->qs, grid * wpb, slots));
+        PK_CUDA(cudaMemsetAsync(h->qs.work, 0, sizeof(int32_t) * 2, s));
+        pk::SearchArgs a{};
+        a.queries = d_q;
+        a.nq = todo;
+        a.qlist = qlist;
+        a.k = k;
+        a.ef = ef_max;
+        a.k_arr = k_arr;
+        a.ef_arr = ef_arr;
+        a.out_stride = stride;
+        a.out_ids = ids;
+        a.out_dists = dists;
+        a.ext0 = h->hg.L[0].ext;
+        a.counters = counters;
+        a.status = h->d_status;
+        a.work = h->qs.work;
+        a.vis = h->qs.vis;
+        a.vis_slots = (int32_t)slots;
+        a.epochs = h->qs.epochs;
+        a.cand_tail = h->qs.cand_tail;
+        a.cand_tail_cap = (int32_t)(slots - pk::kCandTop > 0 ? slots - pk::kCandTop : 0);
+        a.wcap = wcap;
+        const int64_t g = std::min<int64_t>(grid, (todo + wpb - 1) / wpb);
+        PK_CUDA(pk::launch_search_exact(h->dg, h->dtype, h->lc, a, (int)g, wpb, smem, s));
+        int32_t over = 0;
+        PK_CUDA(cudaMemcpyAsync(&over, h->qs.work + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        PK_CUDA(cudaStreamSynchronize(s));
+        if (over == 0) return PK_OK;
+        // rerun the queries that outgrew the scratch with 4x the room
+        std::vector<uint8_t> st(nq);
+        PK_CUDA(cudaMemcpy(st.data(), h->d_status, nq, cudaMemcpyDeviceToHost));
+        std::vector<int32_t> list;
+        for (int64_t i = 0; i < nq; i++)
+            if (st[i]) list.push_back((int32_t)i);
+        PK_TRY(ensure_buf(h, &h->d_qlist, h->qlist_n, (int64_t)list.size()));
+        PK_CUDA(cudaMemcpy(h->d_qlist, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice));
+        PK_CUDA(cudaMemsetAsync(h->d_status, 0, nq, s));
+        qlist = h->d_qlist;
+        todo = (int64_t)list.size();
+        slots *= 4;
+        if (slots > (1LL << 24)) break;
+    }
+    return fail(PK_ERR_OVERFLOW, "search outgrew its scratch after retries");
+}
+
+// Copies nq rows of dim*esz bytes into the padded staging buffer.
+int stage_queries(pk_index *h, const void *q, int64_t nq, cudaMemcpyKind kind, cudaStream_t s) {
+    PK_TRY(ensure_buf(h, &h->d_qstage, h->qstage_rows, nq * h->row_bytes));
+    const size_t w = (size_t)(h->dim * h->esz);
+    if (w != (size_t)h->row_bytes) PK_CUDA(cudaMemsetAsync(h->d_qstage, 0, (size_t)(nq * h->row_bytes), s));
+    PK_CUDA(cudaMemcpy2DAsync(h->d_qstage, (size_t)h->row_bytes, q, w, w, (size_t)nq, kind, s));
+    return PK_OK;
+}
+
+// ---------------------------------------------------------------- insert ----
+
+struct BatchBufs {
+    uint8_t *levels = nullptr;
+    int32_t *ext = nullptr, *top_ins = nullptr, *node_id = nullptr;
+    int32_t *item_node = nullptr, *item_level = nullptr, *item_id = nullptr, *item_down = nullptr;
+    void *out = nullptr;
+    int32_t *counts = nullptr;
+    uint64_t *keys = nullptr;
+    void *edges = nullptr;
+    pk::EdgeWork ew{};
+    int64_t nb_cap = 0, max_levels = 0, top_k0 = 0;
+};
+
+int alloc_batch(pk_index *h, BatchBufs &b, int64_t nb, int64_t max_levels, int64_t top_k0) {
+    b.nb_cap = nb;
+    b.max_levels = max_levels;
+    b.top_k0 = top_k0;
+    const int64_t nl = nb * max_levels, ns = nl * top_k0;
+    PK_TRY(dalloc(h, (void **)&b.levels, nb));
+    PK_TRY(dalloc(h, (void **)&b.ext, 4 * nb));
+    PK_TRY(dalloc(h, (void **)&b.top_ins, 4 * nb));
+    PK_TRY(dalloc(h, (void **)&b.node_id, 4 * nl));
+    PK_TRY(dalloc(h, (void **)&b.item_node, 4 * nl));
+    PK_TRY(dalloc(h, (void **)&b.item_level, 4 * nl));
+    PK_TRY(dalloc(h, (void **)&b.item_id, 4 * nl));
+    PK_TRY(dalloc(h, (void **)&b.item_down, 4 * nl));
+    PK_TRY(dalloc(h, &b.out, 8 * ns));
+    PK_TRY(dalloc(h, (void **)&b.counts, 4 * nl));
+    PK_TRY(dalloc(h, (void **)&b.keys, 8 * ns));
+    PK_TRY(dalloc(h, &b.edges, 8 * ns));
+    b.ew.temp_bytes = pk::edge_sort_temp_bytes(ns);
+    PK_TRY(dalloc(h, &b.ew.temp, b.ew.temp_bytes));
+    PK_TRY(dalloc(h, (void **)&b.ew.keys_sorted, 8 * ns));
+    PK_TRY(dalloc(h, (void **)&b.ew.flags, 4 * ns));
+    PK_TRY(dalloc(h, (void **)&b.ew.scan, 4 * ns));
+    PK_TRY(dalloc(h, (void **)&b.ew.seg_start, 8 * (ns + 1)));
+    PK_TRY(dalloc(h, (void **)&b.ew.nseg, 4));
+    return PK_OK;
+}
+
+void free_batch(pk_index *h, BatchBufs &b) {
+    const int64_t nb = b.nb_cap, nl = nb * b.max_levels, ns = nl * b.top_k0;
+    dfree(h, b.levels, nb);
+    dfree(h, b.ext, 4 * nb);
+    dfree(h, b.top_ins, 4 * nb);
+    dfree(h, b.node_id, 4 * nl);
+    dfree(h, b.item_node, 4 * nl);
+    dfree(h, b.item_level, 4 * nl);
+    dfree(h, b.item_id, 4 * nl);
+    dfree(h, b.item_down, 4 * nl);
+    dfree(h, b.out, 8 * ns);
+    dfree(h, b.counts, 4 * nl);
+    dfree(h, b.keys, 8 * ns);
+    dfree(h, b.edges, 8 * ns);
+    dfree(h, b.ew.temp, b.ew.temp_bytes);
+    dfree(h, b.ew.keys_sorted, 8 * ns);
+    dfree(h, b.ew.flags, 4 * ns);
+    dfree(h, b.ew.scan, 4 * ns);
+    dfree(h, b.ew.seg_start, 8 * (ns + 1));
+    dfree(h, b.ew.nseg, 4);
+    b = BatchBufs{};
+}
+
+// Inserts count rows, row i taken from rows + i*dim*esz with external id
+// ext[i], in that order.
+int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t count, int32_t max_batch) {
+    if (count == 0) return PK_OK;
+    cudaStream_t s = h->stream;
+    const std::vector<double> cp = cumulative_probability(h->M);
+    // levels and bookkeeping
+    int64_t max_ext = -1;
+    for (int64_t i = 0; i < count; i++) {
+        if (ext[i] < 0) return fail(PK_ERR_ARG, "negative external id");
+        max_ext = std::max<int64_t>(max_ext, ext[i]);
+    }
+    if (max_ext >= h->capacity) {
+        h->capacity = max_ext + 1;
+        h->ext_in0.resize(h->capacity, -1);
+        h->ext_level.resize(h->capacity, 0);
+    }
+    std::vector<uint8_t> lv(count);
+    int top = 0;
+    for (int64_t i = 0; i < count; i++) {
+        if (h->ext_in0[ext[i]] >= 0) return fail(PK_ERR_ARG, "external id inserted twice: " + std::to_string(ext[i]));
+        int l;
+        if (!h->level_override.empty()) {
+            if (ext[i] >= (int64_t)h->level_override.size())
+                return fail(PK_ERR_ARG, "no level given for external id " + std::to_string(ext[i]));
+            l = h->level_override[ext[i]];
+        } else {
+            l = draw_level(cp, h->seed, ext[i]);
+        }
+        if (l >= pk::kMaxLayers) return fail(PK_ERR_ARG, "level too high");
+        lv[i] = (uint8_t)l;
+        top = std::max(top, l);
+    }
+    {
+        std::vector<int32_t> sorted(ext, ext + count);
+        std::sort(sorted.begin(), sorted.end());
+        if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+            return fail(PK_ERR_ARG, "duplicate external id in one call");
+    }
+    h->touched = true;
+    // capacity per layer
+    std::vector<int64_t> add_per(top + 1, 0);
+    for (int64_t i = 0; i < count; i++)
+        for (int l = 0; l <= lv[i]; l++) add_per[l]++;
+    const int64_t n0_before = h->n0();
+    for (int l = 0; l <= top; l++) {
+        const int64_t have = l < h->num_layers ? h->hg.L[l].n : 0;
+        PK_TRY(ensure_layer(h, l, have + add_per[l], l == 0 ? 2 * h->M : h->M));
+    }
+    // vectors, in insertion order
+    PK_TRY(ensure_vec(h, n0_before + count));
+    {
+        const int64_t chunk = std::max<int64_t>(1, (256LL << 20) / h->row_bytes);
+        std::vector<uint8_t> tmp;
+        const size_t w = (size_t)(h->dim * h->esz);
+        for (int64_t i0 = 0; i0 < count; i0 += chunk) {
+            const int64_t c = std::min(chunk, count - i0);
+            PK_CUDA(cudaMemcpy2D((uint8_t *)h->hg.vec0 + (n0_before + i0) * h->row_bytes, (size_t)h->row_bytes,
+                                 rows + (size_t)i0 * w, w, w, (size_t)c, cudaMemcpyHostToDevice));
+        }
+    }
+    PK_TRY(push_graph(h));
+
+    // batch buffers
+    const int64_t top_k0 = 2 * h->M;
+    const int64_t max_levels = std::max(top, h->num_layers - 1) + 1;
+    const int wcap = (int)h->efc + 2;
+    int wpb = 4;
+    size_t smem = (size_t)wpb * pk::insert_smem_per_warp(wcap, (int)top_k0);
+    while (wpb > 1 && smem > 200 * 1024) {
+        wpb /= 2;
+        smem = (size_t)wpb * pk::insert_smem_per_warp(wcap, (int)top_k0);
+    }
+    const int bpsm = pk::insert_search_blocks_per_sm(h->dtype, h->lc, wpb, smem);
+    if (bpsm <= 0) return fail(PK_ERR_CUDA, "insert kernel cannot be resident");
+    const int64_t resident = (int64_t)bpsm * h->num_sms * wpb;
+    int64_t bmax = max_batch > 0 ? max_batch : resident;
+    bmax = std::max<int64_t>(1, std::min<int64_t>(bmax, count));
+    BatchBufs bb;
+    PK_TRY(alloc_batch(h, bb, bmax, max_levels, top_k0));
+    struct Guard {
+        pk_index *h;
+        BatchBufs *b;
+        ~Guard() {
+            cudaStreamSynchronize(h->stream);
+            free_batch(h, *b);
+        }
+    } guard{h, &bb};
+    int64_t slots = pow2ceil(std::max<int64_t>(2048, 32LL * h->efc + 2048));
+    // every launched warp owns a scratch slot, including the ones that find
+    // no work: size the scratch by the largest grid this call launches
+    const int64_t max_grid = std::min<int64_t>((bmax + wpb - 1) / wpb, (int64_t)bpsm * h->num_sms);
+    PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, slots));
+
+    const int capmax = (int)top_k0;
+    std::vector<int32_t> node_id, item_node, item_level, item_id, item_down, top_ins, bext;
+    int64_t done = 0, bsize = 1;
+    while (done < count) {
+        const int64_t nb = std::min(std::min(bsize, bmax), count - done);
+        const bool nonempty = h->n0() > 0;
+        const int L = h->hg.enter_level;
+        node_id.assign(nb * max_levels, -1);
+        item_node.clear();
+        item_level.clear();
+        item_id.clear();
+        item_down.clear();
+        top_ins.assign(nb, 0);
+        bext.assign(ext + done, ext + done + nb);
+        std::vector<int64_t> next(max_levels, 0);
+        for (int l = 0; l < max_levels; l++) next[l] = l < h->num_layers ? h->hg.L[l].n : 0;
+        for (int64_t b = 0; b < nb; b++) {
+            const int l = lv[done + b];
+            top_ins[b] = nonempty ? std::min(l, L) : 0;
+            for (int x = 0; x <= l; x++) {
+                const int32_t id = (int32_t)next[x]++;  // NewInID in batch order
+                node_id[b * max_levels + x] = id;
+                item_node.push_back((int32_t)b);
+                item_level.push_back(x);
+                item_id.push_back(id);
+                item_down.push_back(x > 0 ? node_id[b * max_levels + x - 1] : -1);
+            }
+        }
+        PK_CUDA(cudaMemcpyAsync(bb.levels, lv.data() + done, nb, cudaMemcpyHostToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(bb.ext, bext.data(), 4 * nb, cudaMemcpyHostToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(bb.top_ins, top_ins.data(), 4 * nb, cudaMemcpyHostToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(bb.node_id, node_id.data(), 4 * nb * max_levels, cudaMemcpyHostToDevice, s));
+        const int64_t ni = (int64_t)item_node.size();
+        PK_CUDA(cudaMemcpyAsync(bb.item_node, item_node.data(), 4 * ni, cudaMemcpyHostToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(bb.item_level, item_level.data(), 4 * ni, cudaMemcpyHostToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(bb.item_id, item_id.data(), 4 * ni, cudaMemcpyHostToDevice, s));
+        PK_CUDA(cudaMemcpyAsync(bb.item_down, item_down.data(), 4 * ni, cudaMemcpyHostToDevice, s));
+        PK_CUDA(cudaMemsetAsync(bb.counts, 0, 4 * nb * max_levels, s));
+
+        // 1. searches + SelectHeuristic (retried with more scratch on overflow)
+        for (int attempt = 0;; attempt++) {
+            PK_CUDA(cudaMemsetAsync(h->bs.work, 0, sizeof(int32_t) * 2, s));
+            pk::InsertSearchArgs a{};
+            a.nb = (int32_t)nb;
+            a.pos0 = (int32_t)(n0_before + done);
+            a.levels = bb.levels;
+            a.enter_level = L;
+            a.graph_nonempty = nonempty;
+            a.efc = (int32_t)h->efc;
+            a.top_k0 = (int32_t)top_k0;
+            a.max_levels = (int32_t)max_levels;
+            a.out = bb.out;
+            a.counts = bb.counts;
+            a.work = h->bs.work;
+            a.vis = h->bs.vis;
+            a.vis_slots = (int32_t)slots;
+            a.epochs = h->bs.epochs;
+            a.cand_tail = h->bs.cand_tail;
+            a.cand_tail_cap = (int32_t)(slots - pk::kCandTop);
+            a.wcap = wcap;
+            const int64_t grid = std::min<int64_t>((nb + wpb - 1) / wpb, max_grid);
+            PK_CUDA(pk::launch_insert_search(h->dg, h->dtype, h->lc, a, (int)grid, wpb, smem, s));
+            int32_t over = 0;
+            PK_CUDA(cudaMemcpyAsync(&over, h->bs.work + 1, 4, cudaMemcpyDeviceToHost, s));
+            PK_CUDA(cudaStreamSynchronize(s));
+            if (over == 0) break;
+            if (attempt >= 3 || slots >= (1LL << 24)) return fail(PK_ERR_OVERFLOW, "insertion search outgrew scratch");
+            slots *= 4;
+            PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, slots));
+            PK_CUDA(cudaMemsetAsync(bb.counts, 0, 4 * nb * max_levels, s));
+        }
+        // 2. AddNode for every (node, layer)
+        pk::AddNodeArgs na{};
+        na.nitems = ni;
+        na.item_node = bb.item_node;
+        na.item_level = bb.item_level;
+        na.item_id = bb.item_id;
+        na.item_down = bb.item_down;
+        na.ext_ids = bb.ext;
+        na.top_inserted = bb.top_ins;
+        na.pos0 = (int32_t)(n0_before + done);
+        na.max_levels = (int32_t)max_levels;
+        na.top_k0 = (int32_t)top_k0;
+        na.out = bb.out;
+        na.counts = bb.counts;
+        PK_CUDA(pk::launch_add_node(h->dg, na, s));
+        // 3. reverse edges, grouped by target
+        pk::EdgeKeyArgs ka{};
+        ka.nslots = nb * max_levels * top_k0;
+        ka.max_levels = (int32_t)max_levels;
+        ka.top_k0 = (int32_t)top_k0;
+        ka.levels = bb.levels;
+        ka.top_inserted = bb.top_ins;
+        ka.counts = bb.counts;
+        ka.out = bb.out;
+        ka.node_id = bb.node_id;
+        ka.keys = bb.keys;
+        ka.edges = bb.edges;
+        if (nonempty) PK_CUDA(pk::launch_add_edges(h->dg, h->dtype, h->lc, bb.ew, ka, capmax, s));
+        // bookkeeping
+        for (int l = 0; l < max_levels; l++)
+            if (l < h->num_layers) h->hg.L[l].n = next[l];
+        for (int64_t b = 0; b < nb; b++) {
+            h->ext_in0[bext[b]] = (int32_t)node_id[b * max_levels];
+            h->ext_level[bext[b]] = lv[done + b];
+            if (lv[done + b] > h->hg.enter_level) h->hg.enter_level = lv[done + b];
+        }
+        PK_TRY(push_graph(h));
+        done += nb;
+        bsize = std::min<int64_t>(bsize * 2, bmax);
+    }
+    PK_CUDA(cudaStreamSynchronize(s));
+    return PK_OK;
+}
+
+// --------------------------------------------------------------- create -----
+
+int init_handle(pk_index *h, int metric, int dtype, int64_t dim, int64_t M, int64_t efc) {
+    if (metric != PK_METRIC_L2 && metric != PK_METRIC_IP) return fail(PK_ERR_ARG, "metric must be 1 (L2) or 2 (IP)");
+    if (pk::elem_size(dtype) == 0) return fail(PK_ERR_ARG, "dtype must be 0..3");
+    if (dim <= 0 || dim > 65536) return fail(PK_ERR_ARG, "dim out of range");
+    if (M < 2 || M > 4096) return fail(PK_ERR_ARG, "M out of range");
+    if (efc < 1 || efc > 20000) return fail(PK_ERR_ARG, "ef_construction out of range");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(PK_ERR_NO_DEVICE, "no CUDA device");
+    }
+    PK_CUDA(cudaGetDevice(&h->device));
+    PK_CUDA(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+    h->metric = metric;
+    h->dtype = dtype;
+    h->dim = dim;
+    h->M = M;
+    h->efc = efc;
+    h->esz = pk::elem_size(dtype);
+    h->row_bytes = (dim * h->esz + 15) / 16 * 16;
+    h->lc = pk::lane_config(h->row_bytes);
+    PK_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    PK_TRY(dalloc(h, (void **)&h->dg, sizeof(pk::DevGraph)));
+    PK_TRY(dalloc(h, (void **)&h->zero_row, (size_t)h->row_bytes));
+    PK_CUDA(cudaMemset(h->zero_row, 0, (size_t)h->row_bytes));
+    h->hg = pk::DevGraph{};
+    h->hg.zero_row = h->zero_row;
+    h->hg.row_bytes = h->row_bytes;
+    h->hg.dim = (int32_t)dim;
+    h->hg.dtype = dtype;
+    h->hg.metric = metric;
+    h->hg.enter_level = 0;
+    // layer 0 always exists
+    PK_TRY(ensure_layer(h, 0, 0, 2 * M));
+    PK_TRY(ensure_vec(h, 16));
+    PK_TRY(push_graph(h));
+    return PK_OK;
+}
+
+void destroy_handle(pk_index *h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int l = 0; l < h->num_layers; l++) {
+        pk::DevLayer &L = h->hg.L[l];
+        cudaFree(L.adj);
+        cudaFree(L.dist);
+        cudaFree(L.deg);
+        cudaFree(L.heu);
+        cudaFree(L.ext);
+        cudaFree(L.vrow);
+        cudaFree(L.down);
+    }
+    cudaFree((void *)h->hg.vec0);
+    cudaFree(h->zero_row);
+    cudaFree(h->dg);
+    for (SearchScratch *s : {&h->qs, &h->bs}) {
+        cudaFree(s->vis);
+        cudaFree(s->cand_tail);
+        cudaFree(s->epochs);
+        cudaFree(s->work);
+    }
+    cudaFree(h->d_qstage);
+    cudaFree(h->d_ids);
+    cudaFree(h->d_dists);
+    cudaFree(h->d_status);
+    cudaFree(h->d_qlist);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // namespace
+
+// ====================================================================== ABI ==
+
+namespace {
+
+
+static int pk_index_create_impl(pk_index **out, int metric, int dtype, int64_t dim, int64_t M, int64_t ef_construction) {
+    if (!out) return fail(PK_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    pk_index *h = new (std::nothrow) pk_index();
+    if (!h) return fail(PK_ERR_OOM, "host allocation failed");
+    int rc = init_handle(h, metric, dtype, dim, M, ef_construction);
+    if (rc != PK_OK) {
+        destroy_handle(h);
+        return rc;
+    }
+    *out = h;
+    return PK_OK;
+}
+
+static int pk_index_destroy_impl(pk_index *h) {
+    destroy_handle(h);
+    return PK_OK;
+}
+
+static int pk_index_set_seed_impl(pk_index *h, uint64_t seed) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    if (h->touched) return fail(PK_ERR_STATE, "seed must be set before the first insertion");
+    h->seed = seed;
+    return PK_OK;
+}
+
+static int pk_index_set_levels_impl(pk_index *h, const uint8_t *levels, int64_t n) {
+    if (!h || (!levels && n > 0) || n < 0) return fail(PK_ERR_ARG, "bad arguments");
+    if (h->touched) return fail(PK_ERR_STATE, "levels must be set before the first insertion");
+    for (int64_t i = 0; i < n; i++)
+        if (levels[i] >= pk::kMaxLayers) return fail(PK_ERR_ARG, "level too high");
+    h->level_override.assign(levels, levels + n);
+    return PK_OK;
+}
+
+static int pk_index_build_impl(pk_index *h, const void *data, int64_t n, const int32_t *ext_ids, int32_t max_batch) {
+    if (!h || (!data && n > 0) || n < 0) return fail(PK_ERR_ARG, "bad arguments");
+    if (h->n0() > 0) return fail(PK_ERR_STATE, "build needs an empty index");
+    std::vector<int32_t> order(n);
+    for (int64_t i = 0; i < n; i++) {
+        order[i] = ext_ids ? ext_ids[i] : (int32_t)i;
+        if (order[i] < 0 || order[i] >= n) return fail(PK_ERR_ARG, "external ids must lie in [0, n)");
+    }
+    // rows in insertion order: row i is data[order[i]]
+    const size_t w = (size_t)(h->dim * h->esz);
+    std::vector<uint8_t> rows;
+    try {
+        rows.resize((size_t)n * w);
+    } catch (...) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    }
+    const uint8_t *src = static_cast<const uint8_t *>(data);
+    for (int64_t i = 0; i < n; i++) std::memcpy(rows.data() + (size_t)i * w, src + (size_t)order[i] * w, w);
+    if (h->capacity < n) {
+        h->capacity = n;
+        h->ext_in0.resize(n, -1);
+        h->ext_level.resize(n, 0);
+    }
+    return insert_rows(h, rows.data(), order.data(), n, max_batch);
+}
+
+static int pk_index_add_impl(pk_index *h, const void *rows, int64_t n, const int32_t *ext_ids, int32_t max_batch) {
+    if (!h || ((!rows || !ext_ids) && n > 0) || n < 0) return fail(PK_ERR_ARG, "bad arguments");
+    return insert_rows(h, static_cast<const uint8_t *>(rows), ext_ids, n, max_batch);
+}
+
+static int pk_index_search_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
+                    float *out_dists) {
+    if (!h || nq < 0 || ((!queries || !out_ids || !out_dists) && nq > 0)) return fail(PK_ERR_ARG, "bad arguments");
+    if (k < 1 || ef < 1) return fail(PK_ERR_ARG, "k and ef must be >= 1");
+    if (nq == 0) return PK_OK;
+    if (h->n0() == 0) {
+        for (int64_t i = 0; i < nq * k; i++) {
+            out_ids[i] = -1;
+            out_dists[i] = FLT_MAX;
+        }
+        return PK_OK;
+    }
+    cudaStream_t s = h->stream;
+    PK_TRY(stage_queries(h, queries, nq, cudaMemcpyHostToDevice, s));
+    PK_TRY(ensure_buf(h, &h->d_ids, h->ids_n, nq * k));
+    PK_TRY(ensure_buf(h, &h->d_dists, h->dists_n, nq * k));
+    PK_TRY(run_search(h, h->d_qstage, nq, k, ef, nullptr, nullptr, k, h->d_ids, h->d_dists, nullptr, s));
+    PK_CUDA(cudaMemcpyAsync(out_ids, h->d_ids, sizeof(int32_t) * nq * k, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaMemcpyAsync(out_dists, h->d_dists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    return PK_OK;
+}
+
+static int pk_index_search_device_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                           const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride,
+                           int32_t *out_ids, float *out_dists, int32_t *counters, void *stream) {
+    if (!h || nq < 0 || ((!queries || !out_ids || !out_dists) && nq > 0)) return fail(PK_ERR_ARG, "bad arguments");
+    if (k < 1 || ef < 1 || out_stride < k) return fail(PK_ERR_ARG, "need k >= 1, ef >= 1, out_stride >= k");
+    if (nq == 0) return PK_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (h->n0() == 0) {
+        PK_CUDA(fill_i32(out_ids, nq * out_stride, -1, s));
+        PK_CUDA(fill_f32(out_dists, nq * out_stride, FLT_MAX, s));
+        return PK_OK;
+    }
+    const size_t w = (size_t)(h->dim * h->esz);
+    const uint8_t *q = static_cast<const uint8_t *>(queries);
+    if (w != (size_t)h->row_bytes || ((uintptr_t)queries & 15) != 0) {
+        PK_TRY(stage_queries(h, queries, nq, cudaMemcpyDeviceToDevice, s));
+        q = h->d_qstage;
+    }
+    return run_search(h, q, nq, k, ef, k_per_query, ef_per_query, out_stride, out_ids, out_dists, counters, s);
+}
+
+static int pk_index_save_impl(const pk_index *hc, const char *path) {
+    pk_index *h = const_cast<pk_index *>(hc);
+    if (!h || !path) return fail(PK_ERR_ARG, "bad arguments");
+    PK_CUDA(cudaStreamSynchronize(h->stream));
+    pk::FileGraph g;
+    g.metric = h->metric;
+    g.dtype = h->dtype;
+    g.dim = h->dim;
+    g.max_degree = h->M;
+    g.build_ef = h->efc;
+    g.capacity = h->capacity;
+    g.enter_level = h->hg.enter_level;
+    const int nl = h->n0() > 0 ? h->num_layers : 0;
+    g.layers.resize(nl);
+    for (int l = 0; l < nl; l++) {
+        const pk::DevLayer &L = h->hg.L[l];
+        pk::FileLayer &F = g.layers[l];
+        F.n = L.n;
+        F.layer_capacity = std::max(L.lcap, L.n);
+        F.cap = L.cap;
+        F.ent = L.ent;
+        F.ext.resize(F.n);
+        std::vector<int32_t> deg(F.n), heu(F.n), vrow(F.n);
+        F.adj.resize((size_t)(F.layer_capacity * F.cap));
+        F.dist.resize((size_t)(F.layer_capacity * F.cap));
+        PK_CUDA(cudaMemcpy(F.ext.data(), L.ext, 4 * F.n, cudaMemcpyDeviceToHost));
+        PK_CUDA(cudaMemcpy(deg.data(), L.deg, 4 * F.n, cudaMemcpyDeviceToHost));
+        PK_CUDA(cudaMemcpy(heu.data(), L.heu, 4 * F.n, cudaMemcpyDeviceToHost));
+        PK_CUDA(cudaMemcpy(F.adj.data(), L.adj, 4 * F.adj.size(), cudaMemcpyDeviceToHost));
+        PK_CUDA(cudaMemcpy(F.dist.data(), L.dist, 4 * F.dist.size(), cudaMemcpyDeviceToHost));
+        if (l > 0) PK_CUDA(cudaMemcpy(vrow.data(), L.vrow, 4 * F.n, cudaMemcpyDeviceToHost));
+        F.degree.resize(F.n);
+        F.heuristic.resize(F.n);
+        F.has_vector.resize(F.n);
+        for (int64_t i = 0; i < F.n; i++) {
+            F.degree[i] = (int16_t)deg[i];
+            F.heuristic[i] = (int16_t)heu[i];
+            F.has_vector[i] = l == 0 ? 1 : (vrow[i] >= 0 ? 1 : 0);
+        }
+    }
+    const int64_t n0 = h->n0();
+    const size_t w = (size_t)(h->dim * h->esz);
+    g.vectors.resize((size_t)n0 * w);
+    if (n0 > 0)
+        PK_CUDA(cudaMemcpy2D(g.vectors.data(), w, h->hg.vec0, (size_t)h->row_bytes, w, (size_t)n0,
+                             cudaMemcpyDeviceToHost));
+    const int rc = pk::write_graph_file(path, g);
+    if (rc != PK_OK) return fail(rc, std::string("cannot write ") + path);
+    return PK_OK;
+}
+
+static int pk_index_load_impl(pk_index **out, const char *path) {
+    if (!out || !path) return fail(PK_ERR_ARG, "bad arguments");
+    *out = nullptr;
+    pk::FileGraph g;
+    std::string err;
+    int rc = pk::read_graph_file(path, g, err);
+    if (rc != PK_OK) return fail(rc, err);
+    // consistency checks the reference would trip over (ids, ranges)
+    const int nl = (int)g.layers.size();
+    if (nl > pk::kMaxLayers) return fail(PK_ERR_FORMAT, "too many layers");
+    for (int l = 0; l < nl; l++) {
+        const pk::FileLayer &F = g.layers[l];
+        if (F.cap != (l == 0 ? 2 * g.max_degree : g.max_degree)) return fail(PK_ERR_FORMAT, "unexpected layer cap");
+        if (F.n > 0 && (F.ent < 0 || F.ent >= F.layer_capacity)) return fail(PK_ERR_FORMAT, "bad entry id");
+        for (int64_t i = 0; i < F.n; i++) {
+            if (F.ext[i] < 0 || F.ext[i] >= g.capacity) return fail(PK_ERR_FORMAT, "external id out of range");
+            if (F.degree[i] < 0 || F.heuristic[i] < 0) return fail(PK_ERR_FORMAT, "negative degree");
+        }
+    }
+    pk_index *h = new (std::nothrow) pk_index();
+    if (!h) return fail(PK_ERR_OOM, "host allocation failed");
+    rc = init_handle(h, g.metric, g.dtype, g.dim, g.max_degree, g.build_ef);
+    if (rc != PK_OK) {
+        destroy_handle(h);
+        return rc;
+    }
+    auto bail = [&](int code) {
+        destroy_handle(h);
+        return code;
+    };
+    h->touched = true;
+    h->capacity = g.capacity;
+    h->ext_in0.assign(g.capacity, -1);
+    h->ext_level.assign(g.capacity, 0);
+    std::vector<std::vector<int32_t>> ext2in(nl);
+    for (int l = 0; l < nl; l++) {
+        const pk::FileLayer &F = g.layers[l];
+        ext2in[l].assign(g.capacity, -1);
+        for (int64_t i = 0; i < F.n; i++) {
+            ext2in[l][F.ext[i]] = (int32_t)i;
+            h->ext_level[F.ext[i]] = (uint8_t)l;
+        }
+    }
+    if (nl > 0)
+        for (int64_t i = 0; i < g.layers[0].n; i++) h->ext_in0[g.layers[0].ext[i]] = (int32_t)i;
+    for (int l = 0; l < nl; l++) {
+        const pk::FileLayer &F = g.layers[l];
+        // spare rows after the last node so that a spilled list read past the
+        // end meets -1 entries (skipped) rather than unallocated memory
+        int64_t need = F.layer_capacity;
+        for (int64_t i = 0; i < F.n; i++) need = std::max(need, (i * F.cap + F.degree[i] + F.cap - 1) / F.cap);
+        if ((rc = ensure_layer(h, l, need, F.cap)) != PK_OK) return bail(rc);
+        pk::DevLayer &L = h->hg.L[l];
+        L.lcap = F.layer_capacity;
+        L.n = F.n;
+        L.ent = F.ent;
+        std::vector<int32_t> deg(F.n), heu(F.n), vrow(F.n, -1), down(F.n, -1);
+        for (int64_t i = 0; i < F.n; i++) {
+            deg[i] = F.degree[i];
+            heu[i] = F.heuristic[i];
+            if (l > 0) {
+                vrow[i] = F.has_vector[i] ? h->ext_in0[F.ext[i]] : -1;
+                down[i] = ext2in[l - 1][F.ext[i]];
+            }
+        }
+        if (cudaMemcpy(L.ext, F.ext.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.deg, deg.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.heu, heu.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.adj, F.adj.data(), 4 * F.adj.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.dist, F.dist.data(), 4 * F.dist.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            (l > 0 && cudaMemcpy(L.vrow, vrow.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess) ||
+            (l > 0 && cudaMemcpy(L.down, down.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess))
+            return bail(fail(PK_ERR_CUDA, "upload failed"));
+    }
+    const int64_t n0 = nl > 0 ? g.layers[0].n : 0;
+    const int64_t lcap0 = nl > 0 ? g.layers[0].layer_capacity : 0;
+    if ((rc = ensure_vec(h, std::max<int64_t>(lcap0, 1))) != PK_OK) return bail(rc);
+    const size_t w = (size_t)(h->dim * h->esz);
+    if (n0 > 0 && cudaMemcpy2D((void *)h->hg.vec0, (size_t)h->row_bytes, g.vectors.data(), w, w, (size_t)n0,
+                               cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(PK_ERR_CUDA, "vector upload failed"));
+    h->hg.enter_level = nl > 0 ? g.enter_level : 0;
+    if ((rc = push_graph(h)) != PK_OK) return bail(rc);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(PK_ERR_CUDA, "sync failed"));
+    *out = h;
+    return PK_OK;
+}
+
+static int pk_index_info_impl(const pk_index *h, int64_t *out) {
+    if (!h || !out) return fail(PK_ERR_ARG, "bad arguments");
+    out[0] = h->n0();
+    out[1] = h->n0() > 0 ? h->num_layers : 0;
+    out[2] = h->hg.enter_level;
+    out[3] = h->capacity;
+    out[4] = h->dim;
+    out[5] = h->M;
+    out[6] = h->efc;
+    out[7] = h->metric;
+    out[8] = h->dtype;
+    out[9] = (int64_t)h->dev_bytes;
+    out[10] = 2 * h->M;
+    out[11] = h->hg.L[0].ent;
+    return PK_OK;
+}
+
+static int pk_index_layer_impl(const pk_index *hc, int level, int64_t *n, int64_t *layer_capacity, int64_t *cap, int32_t *ext,
+                   int16_t *degree, int16_t *heuristic, uint8_t *has_vector, int32_t *adj, float *dist) {
+    pk_index *h = const_cast<pk_index *>(hc);
+    if (!h || !n || !layer_capacity || !cap) return fail(PK_ERR_ARG, "bad arguments");
+    if (level < 0 || level >= h->num_layers) return fail(PK_ERR_ARG, "no such layer");
+    PK_CUDA(cudaStreamSynchronize(h->stream));
+    const pk::DevLayer &L = h->hg.L[level];
+    *n = L.n;
+    *layer_capacity = std::max(L.lcap, L.n);
+    *cap = L.cap;
+    const int64_t cnt = *layer_capacity * L.cap;
+    if (ext) PK_CUDA(cudaMemcpy(ext, L.ext, 4 * L.n, cudaMemcpyDeviceToHost));
+    std::vector<int32_t> tmp(L.n);
+    if (degree) {
+        PK_CUDA(cudaMemcpy(tmp.data(), L.deg, 4 * L.n, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < L.n; i++) degree[i] = (int16_t)tmp[i];
+    }
+    if (heuristic) {
+        PK_CUDA(cudaMemcpy(tmp.data(), L.heu, 4 * L.n, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < L.n; i++) heuristic[i] = (int16_t)tmp[i];
+    }
+    if (has_vector) {
+        if (level == 0) {
+            for (int64_t i = 0; i < L.n; i++) has_vector[i] = 1;
+        } else {
+            PK_CUDA(cudaMemcpy(tmp.data(), L.vrow, 4 * L.n, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < L.n; i++) has_vector[i] = tmp[i] >= 0;
+        }
+    }
+    if (adj) PK_CUDA(cudaMemcpy(adj, L.adj, 4 * cnt, cudaMemcpyDeviceToHost));
+    if (dist) PK_CUDA(cudaMemcpy(dist, L.dist, 4 * cnt, cudaMemcpyDeviceToHost));
+    return PK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pk_last_error(void) { return g_last_error.c_str(); }
+
+int pk_version(void) { return 100; }
+
+int pk_index_create(pk_index **out, int metric, int dtype, int64_t dim, int64_t M, int64_t ef_construction) {
+    try {
+        return pk_index_create_impl(out, metric, dtype, dim, M, ef_construction);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_create: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_create: unknown exception");
+    }
+}
+
+int pk_index_destroy(pk_index *h) {
+    try {
+        return pk_index_destroy_impl(h);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_destroy: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_destroy: unknown exception");
+    }
+}
+
+int pk_index_set_seed(pk_index *h, uint64_t seed) {
+    try {
+        return pk_index_set_seed_impl(h, seed);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_set_seed: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_set_seed: unknown exception");
+    }
+}
+
+int pk_index_set_levels(pk_index *h, const uint8_t *levels, int64_t n) {
+    try {
+        return pk_index_set_levels_impl(h, levels, n);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_set_levels: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_set_levels: unknown exception");
+    }
+}
+
+int pk_index_build(pk_index *h, const void *data, int64_t n, const int32_t *ext_ids, int32_t max_batch) {
+    try {
+        return pk_index_build_impl(h, data, n, ext_ids, max_batch);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_build: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_build: unknown exception");
+    }
+}
+
+int pk_index_add(pk_index *h, const void *rows, int64_t n, const int32_t *ext_ids, int32_t max_batch) {
+    try {
+        return pk_index_add_impl(h, rows, n, ext_ids, max_batch);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_add: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_add: unknown exception");
+    }
+}
+
+int pk_index_search(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
+                    float *out_dists) {
+    try {
+        return pk_index_search_impl(h, queries, nq, k, ef, out_ids, out_dists);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_search: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_search: unknown exception");
+    }
+}
+
+int pk_index_search_device(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                           const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride,
+                           int32_t *out_ids, float *out_dists, int32_t *counters, void *stream) {
+    try {
+        return pk_index_search_device_impl(h, queries, nq, k, ef, k_per_query, ef_per_query, out_stride, out_ids, out_dists, counters, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_search_device: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_search_device: unknown exception");
+    }
+}
+
+int pk_index_save(const pk_index *hc, const char *path) {
+    try {
+        return pk_index_save_impl(hc, path);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_save: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_save: unknown exception");
+    }
+}
+
+int pk_index_load(pk_index **out, const char *path) {
+    try {
+        return pk_index_load_impl(out, path);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_load: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_load: unknown exception");
+    }
+}
+
+int pk_index_info(const pk_index *h, int64_t *out) {
+    try {
+        return pk_index_info_impl(h, out);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_info: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_info: unknown exception");
+    }
+}
+
+int pk_index_layer(const pk_index *hc, int level, int64_t *n, int64_t *layer_capacity, int64_t *cap, int32_t *ext,
+                   int16_t *degree, int16_t *heuristic, uint8_t *has_vector, int32_t *adj, float *dist) {
+    try {
+        return pk_index_layer_impl(hc, level, n, layer_capacity, cap, ext, degree, heuristic, has_vector, adj, dist);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(PK_ERR_STATE, std::string("pk_index_layer: ") + e.what());
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_layer: unknown exception");
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+"""Device insertion (batched build) against the oracle and the reference.
+
+With one node per batch the device build is the reference's one-thread build
+with adjacency lists bounded by their caps, which the oracle restates as
+GROWTH_CAPPED: on integer data the two graphs must be identical array by
+array.  With large batches the graph differs (nodes of a batch do not see each
+other), and the bar is recall: searching it must reach the recall of a graph
+built by the reference's own code at the same M, ef_construction and ef.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from pickle_b200 import HNSWIndex, datasets
+from tests.helpers import case_data, levels_for
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["f32int_l2", "u8_ip", "i8_l2_d100"])
+def test_one_node_batches_equal_oracle_build(name, gpu):
+    metric, base, queries, M, efc = case_data(name)
+    n = 1500
+    base = base[:n]
+    order = np.random.default_rng(5).permutation(n).astype(np.int32)
+    lv = levels_for(n, M, 5)
+    g = oracle.OraGraph.new(metric, base.dtype, base.shape[1], M, efc, lv, oracle.GROWTH_CAPPED)
+    g.build(base, order)
+    idx = HNSWIndex(base.shape[1], base.dtype, metric, M, efc)
+    idx.set_levels(lv)
+    idx.build(base, order, max_batch=1)
+    info = idx.info()
+    oinfo = g.info()
+    assert info["n"] == oinfo["n0"] and info["num_layers"] == oinfo["num_layers"]
+    assert info["enter_level"] == oinfo["enter_level"]
+    for level in range(oinfo["num_layers"]):
+        a, b = idx.layer(level), g.layer(level)
+        n_l, cap = b["n"], b["cap"]
+        assert a["n"] == n_l and a["cap"] == cap
+        np.testing.assert_array_equal(a["ext"], b["ext"])
+        np.testing.assert_array_equal(a["degree"], b["degree"])
+        np.testing.assert_array_equal(a["heuristic"], b["heuristic"])
+        np.testing.assert_array_equal(a["adj"][:n_l * cap], b["adj"][:n_l * cap])
+        np.testing.assert_array_equal(a["dist"][:n_l * cap], b["dist"][:n_l * cap])
+    # and the two graphs answer queries identically
+    oi, od = g.search(queries, 10, 40)
+    ids, ds = idx.search(queries, 10, 40)
+    np.testing.assert_array_equal(ids, oi)
+    np.testing.assert_array_equal(ds, od)
+
+
+def test_saved_build_reloads_identically(gpu, tmp_path):
+    metric, base, queries, M, efc = case_data("u8_l2")
+    idx = HNSWIndex(base.shape[1], base.dtype, metric, M, efc)
+    idx.set_seed(11)
+    idx.build(base)
+    p = str(tmp_path / "g.pkg")
+    idx.save(p)
+    ids, ds = idx.search(queries, 10, 40)
+    again = HNSWIndex.load(p)
+    i2, d2 = again.search(queries, 10, 40)
+    np.testing.assert_array_equal(ids, i2)
+    np.testing.assert_array_equal(ds, d2)
+    # the oracle reads the device library's file and answers the same
+    g = oracle.OraGraph.load(p)
+    oi, od = g.search(queries, 10, 40)
+    np.testing.assert_array_equal(ids, oi)
+    np.testing.assert_array_equal(ds, od)
+
+
+@pytest.mark.parametrize("name", ["f32int_l2", "f32unit_ip"])
+def test_batched_build_reaches_reference_recall(name, gpu, ref_bin, tmp_path):
+    metric, base, queries, M, efc = case_data(name)
+    n = len(base)
+    gt, _ = datasets.exact_knn(base, queries, 10, metric)
+    rpath = str(tmp_path / "ref.pkg")
+    oracle.ref_build(base, metric, M, efc, rpath, threads=8)
+    idx = HNSWIndex(base.shape[1], base.dtype, metric, M, efc)
+    idx.set_seed(3)
+    idx.build(base)
+    for ef in (16, 32, 64):
+        ri, _, _ = oracle.ref_search(rpath, queries, 10, ef, threads=4)
+        ids, _ = idx.search(queries, 10, ef)
+        r_ref = datasets.recall_at_k(ri, gt, 10)
+        r_dev = datasets.recall_at_k(ids, gt, 10)
+        assert r_dev >= r_ref - 0.02, (ef, r_dev, r_ref)
