@@ -50,10 +50,36 @@ __device__ __forceinline__ int lower_bound_seq(const float *a, int n, float x) {
     return first;
 }
 
+// Rows one dist_rows step covers; occlusion tests run in steps of this many
+// and stop at the first step that finds an occluder, as the reference's loops
+// stop at the first occluder (the outcome, occluded or not, is the same).
+template <int KMAX>
+__device__ __forceinline__ int step_rows(const LaneCfg &lc) {
+    constexpr int U = KMAX <= 1 ? 4 : KMAX <= 2 ? 2 : 1;
+    return U * (32 / lc.G);
+}
+
+// Is any of the rows[0..n) closer to the row in qr than `bound`?  (strict:
+// d < bound).  Warp-uniform.
+template <int DT, int KMAX>
+__device__ __forceinline__ bool any_closer(const VecView &vv, const LaneCfg &lc, const uint4 (&qr)[KMAX], bool ip,
+                                           const int32_t *rows, float *dd, int n, float bound, int lane) {
+    const int step = step_rows<KMAX>(lc);
+    for (int c0 = 0; c0 < n; c0 += step) {
+        const int m = min(step, n - c0);
+        dist_rows<DT, KMAX, false>(vv, lc, qr, ip, rows + c0, dd + c0, m, lane);
+        __syncwarp();
+        bool hit = false;
+        for (int t = lane; t < m; t += 32) hit |= dd[c0 + t] < bound;
+        if (__any_sync(kFull, hit)) return true;
+    }
+    return false;
+}
+
 // SelectHeuristic (include/hnsw.hpp:70-116) with keep_pruned = true, on the
 // result heap W left in ws.wbuf by search_layer.  Writes R then Pruned to
 // out[0..nR+nP) and returns nR | nP << 16.  rrow/rd: shared staging of
-// top_k entries.
+// top_k entries.  v1 is occluded when some kept r has d(v1, r) < d(v1, q).
 template <int DT, int KMAX>
 __device__ int select_heuristic(const VecView &vv, const LaneCfg &lc, uint4 (&qr)[KMAX], bool ip, const DevLayer &L,
                                 bool layer0, int wl, int top_k, WarpScratch &ws, int32_t *rrow, float *rd, Ent *out,
@@ -72,11 +98,7 @@ __device__ int select_heuristic(const VecView &vv, const LaneCfg &lc, uint4 (&qr
         v1.id = __shfl_sync(kFull, v1.id, 0);
         const int32_t v1row = layer0 ? v1.id : L.vrow[v1.id];
         load_regs<KMAX>(qr, vv.row(v1row), lc, lane, false);
-        dist_rows<DT, KMAX, false>(vv, lc, qr, ip, rrow, rd, nR, lane);
-        __syncwarp();
-        bool occl = false;
-        for (int j = lane; j < nR; j += 32) occl |= v1.d > rd[j];
-        occl = __any_sync(kFull, occl);
+        const bool occl = any_closer<DT, KMAX>(vv, lc, qr, ip, rrow, rd, nR, v1.d, lane);
         if (lane == 0) {
             if (!occl) {
                 out[nR] = v1;
@@ -157,9 +179,40 @@ __global__ void __launch_bounds__(128, 4) insert_search_kernel(const DevGraph *_
                 const DevLayer Ly = gp->L[level];
                 const int32_t e0 = have_enter ? enter : Ly.ent;
                 const int top_k = level == 0 ? a.top_k0 : a.top_k0 / 2;
-                const int wl = search_layer<DT, KMAX, false>(vv, lc, qr, ip, Ly, level == 0, e0, a.efc, ws, cnt,
-                                                             full, lane);
+                int wl = search_layer<DT, KMAX, false>(vv, lc, qr, ip, Ly, level == 0, e0, a.efc, ws, cnt, full,
+                                                       lane);
                 if (full) break;
+                // The batch's earlier nodes (j < bi) are not in the graph yet;
+                // offer every one that joins this layer to the result set, as
+                // if the search had reached it.  With one node per batch there
+                // are none, and the insertion is the reference's exactly.
+                {
+                    MaxHeap W{ws.wbuf, wl};
+                    for (int j0 = 0; j0 < bi; j0 += 32) {
+                        const int j = j0 + lane;
+                        const bool ok = j < bi && a.levels[j] >= level;
+                        const unsigned m = __ballot_sync(kFull, ok);
+                        if (ok) {
+                            const int p = __popc(m & ((1u << lane) - 1));
+                            ws.st->id[p] = a.node_id[(int64_t)j * a.max_levels + level];
+                            ws.st->row[p] = a.pos0 + j;
+                        }
+                        __syncwarp();
+                        const int nn = __popc(m);
+                        dist_rows<DT, KMAX, false>(vv, lc, qr, ip, ws.st->row, ws.st->d, nn, lane);
+                        __syncwarp();
+                        if (lane == 0)
+                            for (int t = 0; t < nn; t++) {
+                                const float d = ws.st->d[t];
+                                if (W.len < a.efc || W.a[0].d > d) {
+                                    W.push(Ent{d, ws.st->id[t]});
+                                    if (W.len > a.efc) W.pop();
+                                }
+                            }
+                        __syncwarp();
+                    }
+                    wl = __shfl_sync(kFull, W.len, 0);
+                }
                 Ent *out = reinterpret_cast<Ent *>(a.out) + ((int64_t)bi * a.max_levels + level) * a.top_k0;
                 const int rp = select_heuristic<DT, KMAX>(vv, lc, qr, ip, Ly, level == 0, wl, top_k, ws, rrow, rd,
                                                            out, lane);
@@ -193,12 +246,19 @@ __global__ void add_node_kernel(DevGraph *__restrict__ gp, const AddNodeArgs a) 
     DevLayer &L = gp->L[lv];
     const int64_t base = (int64_t)id * L.cap;
     const bool add = lv <= a.top_inserted[bi];
-    if (lane == 0) {
-        L.ext[id] = a.ext_ids[bi];
-        if (lv > 0) {
-            L.down[id] = a.item_down[w];
-            L.vrow[id] = add ? a.pos0 + bi : -1;
+    if (a.meta_only) {
+        // NewInID bookkeeping, before the batch's searches: external id, the
+        // id one layer down, and which row holds this layer's copy of the
+        // vector (none above the highest layer the node searched,
+        // include/hnsw.hpp:283-297)
+        if (lane == 0) {
+            L.ext[id] = a.ext_ids[bi];
+            if (lv > 0) {
+                L.down[id] = a.item_down[w];
+                L.vrow[id] = add ? a.pos0 + bi : -1;
+            }
         }
+        return;
     }
     int heur = 0, deg = 0;
     if (add) {
@@ -268,11 +328,7 @@ __global__ void __launch_bounds__(128) add_edge_kernel(DevGraph *__restrict__ gp
         load_regs<KMAX>(qr, vv.row(vrow_of(nid)), lc, lane, false);
         for (int i = lane; i < offset; i += 32) rows[i] = vrow_of(adj[i]);
         __syncwarp();
-        dist_rows<DT, KMAX, false>(vv, lc, qr, ip, rows, dd, offset, lane);
-        __syncwarp();
-        bool occl = false;
-        for (int i = lane; i < offset; i += 32) occl |= distance > dd[i];
-        bool ins = !__any_sync(kFull, occl);
+        bool ins = !any_closer<DT, KMAX>(vv, lc, qr, ip, rows, dd, offset, distance, lane);
         if (ins && offset >= cap) ins = false;
         if (!ins) {
             // insert into the distance-sorted pruned suffix
@@ -318,11 +374,7 @@ __global__ void __launch_bounds__(128) add_edge_kernel(DevGraph *__restrict__ gp
             load_regs<KMAX>(qr, vv.row(vrow_of(v1.id)), lc, lane, false);
             for (int i = lane; i < cur_h; i += 32) rows[i] = vrow_of(adj[i]);
             __syncwarp();
-            dist_rows<DT, KMAX, false>(vv, lc, qr, ip, rows, dd, cur_h, lane);
-            __syncwarp();
-            bool close = false;
-            for (int i = lane; i < cur_h; i += 32) close |= dd[i] < v1.d;
-            bool keep = !__any_sync(kFull, close);
+            bool keep = !any_closer<DT, KMAX>(vv, lc, qr, ip, rows, dd, cur_h, v1.d, lane);
             if (keep && cur_h >= cap) keep = false;
             if (lane == 0) {
                 if (keep) {

@@ -19,7 +19,8 @@ struct InsertSearchArgs {
     int32_t graph_nonempty;
     int32_t efc;
     int32_t top_k0;           // 2M (layer 0); upper layers keep M
-    int32_t max_levels;       // stride of out / counts per node
+    int32_t max_levels;       // stride of out / counts / node_id per node
+    const int32_t *node_id;   // [nb * max_levels] each node's new id per layer
     void *out;                // BuildEnt[nb * max_levels * top_k0]: R then Pruned
     int32_t *counts;          // [nb * max_levels]: nR | nP << 16
     int32_t *work;            // [0] node counter, [1] scratch overflows
@@ -31,8 +32,10 @@ struct InsertSearchArgs {
     int32_t wcap;
 };
 
-// Kernel 2: AddNode for each (node, layer <= its level).
+// Kernel 2: AddNode for each (node, layer <= its level).  With meta_only it
+// writes only the node's bookkeeping (run before kernel 1).
 struct AddNodeArgs {
+    int32_t meta_only;
     int64_t nitems;
     const int32_t *item_node;   // batch index
     const int32_t *item_level;

@@ -522,7 +522,9 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
     const int bpsm = pk::insert_search_blocks_per_sm(h->dtype, h->lc, wpb, smem);
     if (bpsm <= 0) return fail(PK_ERR_CUDA, "insert kernel cannot be resident");
     const int64_t resident = (int64_t)bpsm * h->num_sms * wpb;
-    int64_t bmax = max_batch > 0 ? max_batch : resident;
+    // batches are capped: every node also compares itself with all earlier
+    // nodes of its batch, which grows with the square of the batch
+    int64_t bmax = max_batch > 0 ? max_batch : std::min<int64_t>(resident, 4096);
     bmax = std::max<int64_t>(1, std::min<int64_t>(bmax, count));
     BatchBufs bb;
     PK_TRY(alloc_batch(h, bb, bmax, max_levels, top_k0));
@@ -579,6 +581,21 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
         PK_CUDA(cudaMemcpyAsync(bb.item_down, item_down.data(), 4 * ni, cudaMemcpyHostToDevice, s));
         PK_CUDA(cudaMemsetAsync(bb.counts, 0, 4 * nb * max_levels, s));
 
+        pk::AddNodeArgs na{};
+        na.nitems = ni;
+        na.item_node = bb.item_node;
+        na.item_level = bb.item_level;
+        na.item_id = bb.item_id;
+        na.item_down = bb.item_down;
+        na.ext_ids = bb.ext;
+        na.top_inserted = bb.top_ins;
+        na.pos0 = (int32_t)(n0_before + done);
+        na.max_levels = (int32_t)max_levels;
+        na.top_k0 = (int32_t)top_k0;
+        na.out = bb.out;
+        na.counts = bb.counts;
+        na.meta_only = 1;
+        PK_CUDA(pk::launch_add_node(h->dg, na, s));
         // 1. searches + SelectHeuristic (retried with more scratch on overflow)
         for (int attempt = 0;; attempt++) {
             PK_CUDA(cudaMemsetAsync(h->bs.work, 0, sizeof(int32_t) * 2, s));
@@ -591,6 +608,7 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
             a.efc = (int32_t)h->efc;
             a.top_k0 = (int32_t)top_k0;
             a.max_levels = (int32_t)max_levels;
+            a.node_id = bb.node_id;
             a.out = bb.out;
             a.counts = bb.counts;
             a.work = h->bs.work;
@@ -612,19 +630,7 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
             PK_CUDA(cudaMemsetAsync(bb.counts, 0, 4 * nb * max_levels, s));
         }
         // 2. AddNode for every (node, layer)
-        pk::AddNodeArgs na{};
-        na.nitems = ni;
-        na.item_node = bb.item_node;
-        na.item_level = bb.item_level;
-        na.item_id = bb.item_id;
-        na.item_down = bb.item_down;
-        na.ext_ids = bb.ext;
-        na.top_inserted = bb.top_ins;
-        na.pos0 = (int32_t)(n0_before + done);
-        na.max_levels = (int32_t)max_levels;
-        na.top_k0 = (int32_t)top_k0;
-        na.out = bb.out;
-        na.counts = bb.counts;
+        na.meta_only = 0;
         PK_CUDA(pk::launch_add_node(h->dg, na, s));
         // 3. reverse edges, grouped by target
         pk::EdgeKeyArgs ka{};
