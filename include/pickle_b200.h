@@ -114,6 +114,25 @@ int pk_index_search_device(pk_index *h, const void *queries, int64_t nq, int32_t
                            const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride,
                            int32_t *out_ids, float *out_dists, int32_t *counters, void *stream);
 
+/* No counterpart in the reference.  The exact device search of
+ * pk_index_search_device (uniform k and ef, device pointers, asynchronous work
+ * on `stream` but the call waits for it) without any device allocation: for
+ * callers that cannot let a library call cudaMalloc / cudaFree, such as a
+ * serving loop that must not take the allocator's implicit device-wide
+ * synchronisation, or a process whose device memory is already reserved by
+ * another allocator.  All scratch comes from one fixed 64 MiB array in the
+ * library image, held by every GPU that loads the library until exit.
+ * Limits: nq <= 65536 and ef <= 1024 (PK_ERR_ARG beyond them); a query that
+ * outgrows the fixed scratch is not retried (PK_ERR_OVERFLOW; fall back to
+ * pk_index_search_device).  The index's device must be current.  The first
+ * call on a device looks up the array's address there: make it before any
+ * stream capture.  All calls on a device share the array and keep its
+ * contents between calls (the call clears what must start at zero); calls
+ * that overlap on the GPU race on it, so serialise them.  Results equal
+ * pk_index_search_device's. */
+int pk_index_search_noalloc(const pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                            int32_t *out_ids, float *out_dists, void *stream);
+
 /* Replaces the Serializer::to_disk / from_disk pair that the reference names
  * for persistence (include/serializer.hpp:21-25) but only implements for its
  * retired v0 layer.  Writes / reads the v2 graph file (format described in

@@ -1042,6 +1042,25 @@ static int pk_index_layer_impl(const pk_index *hc, int level, int64_t *n, int64_
 
 }  // namespace
 
+namespace pk {
+// Read-only view of a handle for entry points defined in other files.
+IndexView index_view(const pk_index *h) {
+    IndexView v{};
+    v.device = h->device;
+    v.num_sms = h->num_sms;
+    v.dtype = h->dtype;
+    v.dim = h->dim;
+    v.esz = h->esz;
+    v.row_bytes = h->row_bytes;
+    v.lc = h->lc;
+    v.dg = h->dg;
+    v.ext0 = h->hg.L[0].ext;
+    v.n0 = h->n0();
+    return v;
+}
+void set_error(const char *msg) { g_last_error = msg; }
+}  // namespace pk
+
 extern "C" {
 
 const char *pk_last_error(void) { return g_last_error.c_str(); }

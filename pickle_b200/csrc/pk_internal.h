@@ -121,4 +121,19 @@ __host__ __device__ inline int search_smem_per_warp(int wcap) {
     return ((wcap + kCandTop) * 8 + kStageBytes + 15) & ~15;
 }
 
+// A read-only view of an index handle (pk_index.cu), for entry points
+// defined outside that file.
+struct IndexView {
+    int device;
+    int num_sms;
+    int dtype;
+    int64_t dim, esz, row_bytes;
+    LaneCfg lc;
+    const DevGraph *dg;
+    const int32_t *ext0;
+    int64_t n0;
+};
+IndexView index_view(const pk_index *h);
+void set_error(const char *msg);
+
 }  // namespace pk
