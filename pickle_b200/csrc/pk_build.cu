@@ -131,22 +131,18 @@ __global__ void __launch_bounds__(128, 4) insert_search_kernel(const DevGraph *_
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const int gwarp = blockIdx.x * wpb + wib;
-    unsigned char *my = smem + (size_t)wib * insert_smem_per_warp(a.wcap, a.top_k0);
+    const int64_t row_bytes = gp->row_bytes;
+    unsigned char *my = smem + (size_t)wib * insert_smem_per_warp(a.wcap, a.top_k0, row_bytes);
 
     WarpScratch ws;
     ws.wbuf = reinterpret_cast<Ent *>(my);
     ws.wcap = a.wcap;
     ws.ctop = ws.wbuf + a.wcap;
-    ws.st = reinterpret_cast<Stage *>(ws.ctop + kCandTop);
-    int32_t *rrow = reinterpret_cast<int32_t *>(reinterpret_cast<unsigned char *>(ws.st) + kStageBytes);
+    ws.st = reinterpret_cast<Stage *>(my + search_stage_off(a.wcap));
+    ws.rowbuf = reinterpret_cast<uint8_t *>(my + search_rowbuf_off(a.wcap));
+    int32_t *rrow = reinterpret_cast<int32_t *>(ws.rowbuf + kStageRows * row_bytes);
     float *rd = reinterpret_cast<float *>(rrow + a.top_k0);
-    ws.ctail = reinterpret_cast<Ent *>(a.cand_tail) + (size_t)gwarp * a.cand_tail_cap;
-    ws.ccap = kCandTop + a.cand_tail_cap;
-    ws.vis = a.vis + (size_t)gwarp * a.vis_slots;
-    ws.vmask = (uint32_t)a.vis_slots - 1;
-    ws.vshift = 32 - (__ffs(a.vis_slots) - 1);
-    ws.vlimit = (uint32_t)a.vis_slots / 4 * 3;
-    ws.epoch = a.epochs[gwarp];
+    ws.bind(a.gs, gwarp);
 
     const VecView vv{gp->vec0, gp->zero_row, gp->row_bytes};
     const bool ip = gp->metric == PK_METRIC_IP;
@@ -231,7 +227,6 @@ __global__ void __launch_bounds__(128, 4) insert_search_kernel(const DevGraph *_
         if (full && lane == 0) atomicAdd(a.work + 1, 1);
         __syncwarp();
     }
-    if (lane == 0) a.epochs[gwarp] = ws.epoch;
 }
 
 // AddNode (include/hnsw_layer.hpp:297-332) and the bookkeeping of NewInID

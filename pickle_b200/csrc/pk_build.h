@@ -24,11 +24,7 @@ struct InsertSearchArgs {
     void *out;                // BuildEnt[nb * max_levels * top_k0]: R then Pruned
     int32_t *counts;          // [nb * max_levels]: nR | nP << 16
     int32_t *work;            // [0] node counter, [1] scratch overflows
-    unsigned long long *vis;
-    int32_t vis_slots;
-    uint32_t *epochs;
-    void *cand_tail;
-    int32_t cand_tail_cap;
+    WarpGlobalScratch gs;
     int32_t wcap;
 };
 
@@ -79,8 +75,8 @@ struct EdgeWork {
     int32_t *nseg;
 };
 
-__host__ __device__ inline int insert_smem_per_warp(int wcap, int top_k0) {
-    return search_smem_per_warp(wcap) + ((top_k0 * 8 + 15) & ~15);
+__host__ __device__ inline int insert_smem_per_warp(int wcap, int top_k0, int64_t row_bytes) {
+    return search_smem_per_warp(wcap, row_bytes) + align16((int64_t)top_k0 * 8);
 }
 __host__ __device__ inline int add_edge_smem_per_warp(int capmax) {
     return (((capmax + 2) * 8) * 2 + (capmax + 2) * 4 * 2 + 15) & ~15;

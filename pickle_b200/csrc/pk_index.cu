@@ -84,14 +84,20 @@ inline uint64_t splitmix64(uint64_t &s) {
     return z ^ (z >> 31);
 }
 
-// Scratch of one kind of search launch (queries, or insertion searches).
+// Scratch of one kind of search launch (queries, or insertion searches):
+// per warp a visited bitmap, a list of marked ids, and a candidate-heap spill.
 struct SearchScratch {
     int64_t warps = 0;
-    int64_t slots = 0;      // visited-table slots per warp
-    unsigned long long *vis = nullptr;
-    uint32_t *epochs = nullptr;
+    int64_t bm_words = 0;
+    int64_t vl_cap = 0;
+    int64_t tail_cap = 0;
+    uint32_t *bitmap = nullptr;
+    int32_t *vlist = nullptr;
     void *cand_tail = nullptr;
     int32_t *work = nullptr;
+    pk::WarpGlobalScratch view() const {
+        return pk::WarpGlobalScratch{bitmap, bm_words, vlist, (int32_t)vl_cap, cand_tail, (int32_t)tail_cap};
+    }
 };
 
 }  // namespace
@@ -237,28 +243,36 @@ int ensure_vec(pk_index *h, int64_t rows) {
 }
 
 void free_scratch(pk_index *h, SearchScratch &s) {
-    dfree(h, s.vis, sizeof(unsigned long long) * s.warps * s.slots);
-    dfree(h, s.cand_tail, 8 * (size_t)s.warps * (size_t)s.slots);
-    dfree(h, s.epochs, sizeof(uint32_t) * s.warps);
+    dfree(h, s.bitmap, 4 * (size_t)s.warps * (size_t)s.bm_words);
+    dfree(h, s.vlist, 4 * (size_t)s.warps * (size_t)s.vl_cap);
+    dfree(h, s.cand_tail, 8 * (size_t)s.warps * (size_t)s.tail_cap);
     dfree(h, s.work, sizeof(int32_t) * 4);
     s = SearchScratch{};
 }
 
-int ensure_scratch(pk_index *h, SearchScratch &s, int64_t warps, int64_t slots) {
-    if (s.warps >= warps && s.slots == slots && s.vis) return PK_OK;
-    const int64_t w = std::max(warps, s.slots == slots ? s.warps : (int64_t)0);
-    if (s.vis) {
+// At least `warps` warps of scratch with bitmaps of bm_words words, lists of
+// vl_cap ids and candidate spills of tail_cap entries.  Bitmaps start zeroed
+// and every layer search leaves them zeroed.
+int ensure_scratch(pk_index *h, SearchScratch &s, int64_t warps, int64_t bm_words, int64_t vl_cap, int64_t tail_cap) {
+    if (s.bitmap && s.warps >= warps && s.bm_words >= bm_words && s.vl_cap >= vl_cap && s.tail_cap >= tail_cap)
+        return PK_OK;
+    const int64_t w = std::max(warps, s.warps), bw = std::max(bm_words, s.bm_words);
+    const int64_t vc = std::max(vl_cap, s.vl_cap), tc = std::max(tail_cap, s.tail_cap);
+    if (s.bitmap) {
         PK_CUDA(cudaStreamSynchronize(h->stream));
+        PK_CUDA(cudaDeviceSynchronize());
         free_scratch(h, s);
     }
-    PK_TRY(dalloc(h, (void **)&s.vis, sizeof(unsigned long long) * w * slots));
-    PK_TRY(dalloc(h, &s.cand_tail, 8 * (size_t)w * (size_t)slots));
-    PK_TRY(dalloc(h, (void **)&s.epochs, sizeof(uint32_t) * w));
+    PK_TRY(dalloc(h, (void **)&s.bitmap, 4 * (size_t)w * (size_t)bw));
+    PK_TRY(dalloc(h, (void **)&s.vlist, 4 * (size_t)w * (size_t)vc));
+    PK_TRY(dalloc(h, &s.cand_tail, 8 * (size_t)w * (size_t)tc));
     PK_TRY(dalloc(h, (void **)&s.work, sizeof(int32_t) * 4));
-    PK_CUDA(cudaMemsetAsync(s.vis, 0, sizeof(unsigned long long) * w * slots, h->stream));
-    PK_CUDA(cudaMemsetAsync(s.epochs, 0, sizeof(uint32_t) * w, h->stream));
+    PK_CUDA(cudaMemsetAsync(s.bitmap, 0, 4 * (size_t)w * (size_t)bw, h->stream));
+    PK_CUDA(cudaStreamSynchronize(h->stream));
     s.warps = w;
-    s.slots = slots;
+    s.bm_words = bw;
+    s.vl_cap = vc;
+    s.tail_cap = tc;
     return PK_OK;
 }
 
@@ -312,10 +326,10 @@ int run_search(pk_index *h, const uint8_t *d_q, int64_t nq, int32_t k, int32_t e
     const int ef_max = std::max(ef, 1);
     const int wcap = ef_max + 2;
     int wpb = 4;
-    size_t smem = (size_t)wpb * pk::search_smem_per_warp(wcap);
+    size_t smem = (size_t)wpb * pk::search_smem_per_warp(wcap, h->row_bytes);
     while (wpb > 1 && smem > 200 * 1024) {
         wpb /= 2;
-        smem = (size_t)wpb * pk::search_smem_per_warp(wcap);
+        smem = (size_t)wpb * pk::search_smem_per_warp(wcap, h->row_bytes);
     }
     if (smem > 220 * 1024) return fail(PK_ERR_ARG, "ef too large for shared memory: " + std::to_string(ef));
     const int nb = pk::search_blocks_per_sm(h->dtype, h->lc, wpb, smem);
@@ -323,11 +337,13 @@ int run_search(pk_index *h, const uint8_t *d_q, int64_t nq, int32_t k, int32_t e
     const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + wpb - 1) / wpb);
     PK_TRY(ensure_buf(h, &h->d_status, h->status_n, nq));
 
-    int64_t slots = pow2ceil(std::max<int64_t>(2048, 32LL * ef_max + 2048));
+    const int64_t bm_words = (h->hg.L[0].lcap + 31) / 32 + 1;
+    const int64_t vl_cap = std::max<int64_t>(8192, 64LL * ef_max);
+    int64_t tail = std::max<int64_t>(4096, 32LL * ef_max);
     const int32_t *qlist = nullptr;
     int64_t todo = nq;
     for (int attempt = 0; attempt < 4; attempt++) {
-        PK_TRY(ensure_scratch(h, h->qs, grid * wpb, slots));
+        PK_TRY(ensure_scratch(h, h->qs, grid * wpb, bm_words, vl_cap, tail));
         PK_CUDA(cudaMemsetAsync(h->qs.work, 0, sizeof(int32_t) * 2, s));
         pk::SearchArgs a{};
         a.queries = d_q;
@@ -344,11 +360,7 @@ int run_search(pk_index *h, const uint8_t *d_q, int64_t nq, int32_t k, int32_t e
         a.counters = counters;
         a.status = h->d_status;
         a.work = h->qs.work;
-        a.vis = h->qs.vis;
-        a.vis_slots = (int32_t)slots;
-        a.epochs = h->qs.epochs;
-        a.cand_tail = h->qs.cand_tail;
-        a.cand_tail_cap = (int32_t)(slots - pk::kCandTop > 0 ? slots - pk::kCandTop : 0);
+        a.gs = h->qs.view();
         a.wcap = wcap;
         const int64_t g = std::min<int64_t>(grid, (todo + wpb - 1) / wpb);
         PK_CUDA(pk::launch_search_exact(h->dg, h->dtype, h->lc, a, (int)g, wpb, smem, s));
@@ -356,7 +368,7 @@ int run_search(pk_index *h, const uint8_t *d_q, int64_t nq, int32_t k, int32_t e
         PK_CUDA(cudaMemcpyAsync(&over, h->qs.work + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         PK_CUDA(cudaStreamSynchronize(s));
         if (over == 0) return PK_OK;
-        // rerun the queries that outgrew the scratch with 4x the room
+        // rerun the queries whose candidate heap outgrew its spill, with 4x the room
         std::vector<uint8_t> st(nq);
         PK_CUDA(cudaMemcpy(st.data(), h->d_status, nq, cudaMemcpyDeviceToHost));
         std::vector<int32_t> list;
@@ -367,8 +379,8 @@ int run_search(pk_index *h, const uint8_t *d_q, int64_t nq, int32_t k, int32_t e
         PK_CUDA(cudaMemsetAsync(h->d_status, 0, nq, s));
         qlist = h->d_qlist;
         todo = (int64_t)list.size();
-        slots *= 4;
-        if (slots > (1LL << 24)) break;
+        tail *= 4;
+        if (tail > (1LL << 24)) break;
     }
     return fail(PK_ERR_OVERFLOW, "search outgrew its scratch after retries");
 }
@@ -514,10 +526,10 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
     const int64_t max_levels = std::max(top, h->num_layers - 1) + 1;
     const int wcap = (int)h->efc + 2;
     int wpb = 4;
-    size_t smem = (size_t)wpb * pk::insert_smem_per_warp(wcap, (int)top_k0);
+    size_t smem = (size_t)wpb * pk::insert_smem_per_warp(wcap, (int)top_k0, h->row_bytes);
     while (wpb > 1 && smem > 200 * 1024) {
         wpb /= 2;
-        smem = (size_t)wpb * pk::insert_smem_per_warp(wcap, (int)top_k0);
+        smem = (size_t)wpb * pk::insert_smem_per_warp(wcap, (int)top_k0, h->row_bytes);
     }
     const int bpsm = pk::insert_search_blocks_per_sm(h->dtype, h->lc, wpb, smem);
     if (bpsm <= 0) return fail(PK_ERR_CUDA, "insert kernel cannot be resident");
@@ -536,11 +548,13 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
             free_batch(h, *b);
         }
     } guard{h, &bb};
-    int64_t slots = pow2ceil(std::max<int64_t>(2048, 32LL * h->efc + 2048));
     // every launched warp owns a scratch slot, including the ones that find
     // no work: size the scratch by the largest grid this call launches
     const int64_t max_grid = std::min<int64_t>((bmax + wpb - 1) / wpb, (int64_t)bpsm * h->num_sms);
-    PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, slots));
+    const int64_t bm_words = (h->hg.L[0].lcap + 31) / 32 + 1;
+    const int64_t vl_cap = std::max<int64_t>(8192, 64LL * h->efc);
+    int64_t tail = std::max<int64_t>(4096, 32LL * h->efc);
+    PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, bm_words, vl_cap, tail));
 
     const int capmax = (int)top_k0;
     std::vector<int32_t> node_id, item_node, item_level, item_id, item_down, top_ins, bext;
@@ -612,11 +626,7 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
             a.out = bb.out;
             a.counts = bb.counts;
             a.work = h->bs.work;
-            a.vis = h->bs.vis;
-            a.vis_slots = (int32_t)slots;
-            a.epochs = h->bs.epochs;
-            a.cand_tail = h->bs.cand_tail;
-            a.cand_tail_cap = (int32_t)(slots - pk::kCandTop);
+            a.gs = h->bs.view();
             a.wcap = wcap;
             const int64_t grid = std::min<int64_t>((nb + wpb - 1) / wpb, max_grid);
             PK_CUDA(pk::launch_insert_search(h->dg, h->dtype, h->lc, a, (int)grid, wpb, smem, s));
@@ -624,9 +634,9 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
             PK_CUDA(cudaMemcpyAsync(&over, h->bs.work + 1, 4, cudaMemcpyDeviceToHost, s));
             PK_CUDA(cudaStreamSynchronize(s));
             if (over == 0) break;
-            if (attempt >= 3 || slots >= (1LL << 24)) return fail(PK_ERR_OVERFLOW, "insertion search outgrew scratch");
-            slots *= 4;
-            PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, slots));
+            if (attempt >= 3 || tail >= (1LL << 24)) return fail(PK_ERR_OVERFLOW, "insertion search outgrew scratch");
+            tail *= 4;
+            PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, bm_words, vl_cap, tail));
             PK_CUDA(cudaMemsetAsync(bb.counts, 0, 4 * nb * max_levels, s));
         }
         // 2. AddNode for every (node, layer)
@@ -719,9 +729,9 @@ void destroy_handle(pk_index *h) {
     cudaFree(h->zero_row);
     cudaFree(h->dg);
     for (SearchScratch *s : {&h->qs, &h->bs}) {
-        cudaFree(s->vis);
+        cudaFree(s->bitmap);
+        cudaFree(s->vlist);
         cudaFree(s->cand_tail);
-        cudaFree(s->epochs);
         cudaFree(s->work);
     }
     cudaFree(h->d_qstage);
@@ -1056,6 +1066,7 @@ IndexView index_view(const pk_index *h) {
     v.dg = h->dg;
     v.ext0 = h->hg.L[0].ext;
     v.n0 = h->n0();
+    v.lcap0 = h->hg.L[0].lcap;
     return v;
 }
 void set_error(const char *msg) { g_last_error = msg; }

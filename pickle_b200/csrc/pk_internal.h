@@ -86,6 +86,17 @@ inline int64_t elem_size(int dtype) {
     }
 }
 
+// Global scratch of the search warps: per warp a visited bitmap, the list of
+// ids marked in the current layer search, and the spill of the candidate heap.
+struct WarpGlobalScratch {
+    uint32_t *bitmap;           // warps * bm_words
+    int64_t bm_words;           // >= layer-0 capacity / 32
+    int32_t *vlist;             // warps * vl_cap
+    int32_t vl_cap;
+    void *cand_tail;            // warps * cand_tail_cap entries of 8 bytes
+    int32_t cand_tail_cap;
+};
+
 // Search launch parameters (see pk_search.cu).
 struct SearchArgs {
     const uint8_t *queries;     // nq rows of row_bytes (padded staging copy)
@@ -100,11 +111,7 @@ struct SearchArgs {
     int32_t *counters;          // nq * 6 or null
     uint8_t *status;            // nq: 0 done, 1 scratch overflow (retry)
     int32_t *work;              // [0] work counter, [1] overflow count
-    unsigned long long *vis;    // per-warp visited tables
-    int32_t vis_slots;          // power of two
-    uint32_t *epochs;           // per-warp epoch counters
-    void *cand_tail;            // per-warp candidate-heap spill
-    int32_t cand_tail_cap;
+    WarpGlobalScratch gs;
     int32_t wcap;               // result-heap capacity in shared memory
 };
 
@@ -113,12 +120,18 @@ struct SearchArgs {
 int search_blocks_per_sm(int dtype, const LaneCfg &lc, int warps_per_block, size_t smem);
 cudaError_t launch_search_exact(const DevGraph *g, int dtype, const LaneCfg &lc, const SearchArgs &a, int grid,
                                 int warps_per_block, size_t smem, cudaStream_t s);
-constexpr int kCandTop = 512;   // candidate-heap entries kept in shared memory
+constexpr int kCandTop = 256;   // candidate-heap entries kept in shared memory
 constexpr int kStageBytes = 32 * 4 * 3;  // per-warp staging of one adjacency chunk
+constexpr int kStageRows = 16;           // vector rows staged in shared memory at once
 // Shared memory of one search warp: result heap (wcap entries of 8 bytes),
-// top of the candidate heap, staging.
-__host__ __device__ inline int search_smem_per_warp(int wcap) {
-    return ((wcap + kCandTop) * 8 + kStageBytes + 15) & ~15;
+// top of the candidate heap, staging of one adjacency chunk (ids, rows,
+// distances), then kStageRows vector rows.  Every region starts on a 16-byte
+// boundary: the row buffer is read and written with 16-byte accesses.
+__host__ __device__ inline int align16(int64_t x) { return (int)((x + 15) & ~(int64_t)15); }
+__host__ __device__ inline int search_stage_off(int wcap) { return align16((int64_t)(wcap + kCandTop) * 8); }
+__host__ __device__ inline int search_rowbuf_off(int wcap) { return search_stage_off(wcap) + kStageBytes; }
+__host__ __device__ inline int search_smem_per_warp(int wcap, int64_t row_bytes) {
+    return align16(search_rowbuf_off(wcap) + kStageRows * row_bytes);
 }
 
 // A read-only view of an index handle (pk_index.cu), for entry points
@@ -132,6 +145,7 @@ struct IndexView {
     const DevGraph *dg;
     const int32_t *ext0;
     int64_t n0;
+    int64_t lcap0;  // layer-0 capacity: ids stay below it
 };
 IndexView index_view(const pk_index *h);
 void set_error(const char *msg);

@@ -22,11 +22,13 @@
 //    (with that device current); make that first call before any stream
 //    capture begins.
 //  * Every call on a device shares the one array, which keeps the previous
-//    call's contents.  The parts that must start from zero (work counters,
-//    and the visited tables whenever their layout changes) are cleared by the
-//    call itself.  Calls that overlap on the GPU (two streams, two threads,
-//    two indexes on the same device) race on the array and give wrong
-//    results: serialise them.
+//    call's contents.  What must start from zero is cleared by the call: the
+//    work counters on every call, and the visited bitmaps, which sit at the
+//    front of the array: a completed search leaves its bitmaps all-zero, so a
+//    call clears only the part of its bitmap area that reaches beyond the area
+//    the previous calls on this device left clean.  Calls that overlap on the
+//    GPU (two streams, two threads, two indexes on the same device) race on
+//    the array and give wrong results: serialise them.
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
@@ -49,9 +51,8 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 std::mutex g_mu;
 unsigned char *g_scratch_addr[kMaxDevices] = {};
-// layout of the visited tables at the last call on each device: a change
-// moves the per-warp slot boundaries, so the tables are cleared
-int64_t g_last_layout[kMaxDevices][3] = {};
+// bytes at the front of the bitmap area known to be zero on each device
+size_t g_clean_bytes[kMaxDevices] = {};
 
 __global__ void noalloc_fill_kernel(int32_t *ids, float *d, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -110,51 +111,55 @@ int search_noalloc(const pk_index *h, const void *queries, int64_t nq, int32_t k
     // kernel shape, as pk_index_search_device chooses it
     const int wcap = ef + 2;
     int wpb = 4;
-    size_t smem = (size_t)wpb * pk::search_smem_per_warp(wcap);
+    size_t smem = (size_t)wpb * pk::search_smem_per_warp(wcap, v.row_bytes);
     while (wpb > 1 && smem > 200 * 1024) {
         wpb /= 2;
-        smem = (size_t)wpb * pk::search_smem_per_warp(wcap);
+        smem = (size_t)wpb * pk::search_smem_per_warp(wcap, v.row_bytes);
     }
     const int nb = pk::search_blocks_per_sm(v.dtype, v.lc, wpb, smem);
     if (nb <= 0) return fail(PK_ERR_CUDA, "pk_index_search_noalloc: search kernel cannot be resident");
-    int64_t slots = 1;
-    while (slots < 32LL * ef + 2048) slots <<= 1;
+    const int64_t bm_words = (v.lcap0 + 31) / 32 + 1;
+    const int64_t vl_cap = std::max<int64_t>(4096, 16LL * ef);
+    const int64_t tail = std::max<int64_t>(4096, 32LL * ef);
 
-    // carve the array: counters | status | staged queries | epochs | tables | spill
+    // carve the array: counters | bitmaps | status | staged queries | id lists | spills
     const bool stage = (v.dim * v.esz) != v.row_bytes || (reinterpret_cast<uintptr_t>(queries) & 15) != 0;
-    size_t off = 256;  // work counters
+    const size_t bm_off = 256;  // after the work counters
+    size_t fixed = align256((size_t)nq) + (stage ? align256((size_t)nq * (size_t)v.row_bytes) : 0) + 256 * 4;
+    const size_t per_warp = (size_t)bm_words * 4 + (size_t)vl_cap * 4 + (size_t)tail * 8;
+    if (bm_off + fixed >= kNoAllocScratchBytes)
+        return fail(PK_ERR_ARG, "pk_index_search_noalloc: the queries do not fit the fixed scratch");
+    int64_t warps = (int64_t)((kNoAllocScratchBytes - bm_off - fixed) / per_warp);
+    warps = std::min<int64_t>(warps, (int64_t)nb * v.num_sms * wpb);
+    warps = std::min<int64_t>(warps, (nq + wpb - 1) / wpb * wpb);
+    warps = warps / wpb * wpb;
+    if (warps < wpb)
+        return fail(PK_ERR_ARG, "pk_index_search_noalloc: the index or ef is too large for the fixed scratch");
+    const size_t bm_bytes = (size_t)warps * (size_t)bm_words * 4;
+    size_t off = align256(bm_off + bm_bytes);
     const size_t status_off = off;
     off = align256(off + (size_t)nq);
     const size_t qstage_off = off;
     if (stage) off = align256(off + (size_t)nq * (size_t)v.row_bytes);
-    const size_t per_warp = (size_t)slots * 8 + (size_t)(slots - pk::kCandTop) * 8 + 4;
-    if (off + 256 * 3 >= kNoAllocScratchBytes)
-        return fail(PK_ERR_ARG, "pk_index_search_noalloc: the queries do not fit the fixed scratch");
-    int64_t warps = (int64_t)((kNoAllocScratchBytes - off - 256 * 3) / per_warp);
-    warps = std::min<int64_t>(warps, (int64_t)nb * v.num_sms * wpb);
-    warps = std::min<int64_t>(warps, (nq + wpb - 1) / wpb * wpb);
-    warps = warps / wpb * wpb;
-    if (warps < wpb) return fail(PK_ERR_ARG, "pk_index_search_noalloc: ef too large for the fixed scratch");
-    const size_t epochs_off = off;
-    off = align256(off + (size_t)warps * 4);
-    const size_t vis_off = off;
-    off = align256(off + (size_t)warps * (size_t)slots * 8);
+    const size_t vl_off = off;
+    off = align256(off + (size_t)warps * (size_t)vl_cap * 4);
     const size_t tail_off = off;
-    off += (size_t)warps * (size_t)(slots - pk::kCandTop) * 8;
+    off += (size_t)warps * (size_t)tail * 8;
     if (off > kNoAllocScratchBytes) return fail(PK_ERR_ARG, "pk_index_search_noalloc: scratch layout overflow");
 
-    // what must start at zero
+    // what must start at zero: the counters, and the bitmaps beyond the part
+    // that earlier calls left clean
     if (cudaMemsetAsync(base, 0, 256, s) != cudaSuccess) return fail(PK_ERR_CUDA, "memset of counters failed");
     {
         std::lock_guard<std::mutex> lock(g_mu);
-        int64_t *last = g_last_layout[v.device];
-        if (last[0] != slots || last[1] != warps || last[2] != (int64_t)vis_off) {
-            if (cudaMemsetAsync(base + epochs_off, 0, tail_off - epochs_off, s) != cudaSuccess)
-                return fail(PK_ERR_CUDA, "memset of visited tables failed");
-            last[0] = slots;
-            last[1] = warps;
-            last[2] = (int64_t)vis_off;
+        size_t &clean = g_clean_bytes[v.device];
+        if (bm_bytes > clean) {
+            if (cudaMemsetAsync(base + bm_off + clean, 0, bm_bytes - clean, s) != cudaSuccess)
+                return fail(PK_ERR_CUDA, "pk_index_search_noalloc: clearing the visited bitmaps failed");
         }
+        // after this call only its own bitmap area is known to be clean: the
+        // regions behind it are overwritten by the lists, spills and staging
+        clean = bm_bytes;
     }
     const uint8_t *q = static_cast<const uint8_t *>(queries);
     if (stage) {
@@ -181,11 +186,9 @@ int search_noalloc(const pk_index *h, const void *queries, int64_t nq, int32_t k
     a.counters = nullptr;
     a.status = base + status_off;
     a.work = reinterpret_cast<int32_t *>(base);
-    a.vis = reinterpret_cast<unsigned long long *>(base + vis_off);
-    a.vis_slots = (int32_t)slots;
-    a.epochs = reinterpret_cast<uint32_t *>(base + epochs_off);
-    a.cand_tail = base + tail_off;
-    a.cand_tail_cap = (int32_t)(slots - pk::kCandTop);
+    a.gs = pk::WarpGlobalScratch{reinterpret_cast<uint32_t *>(base + bm_off), bm_words,
+                                 reinterpret_cast<int32_t *>(base + vl_off), (int32_t)vl_cap, base + tail_off,
+                                 (int32_t)tail};
     a.wcap = wcap;
     cudaError_t e = pk::launch_search_exact(v.dg, v.dtype, v.lc, a, (int)(warps / wpb), wpb, smem, s);
     if (e != cudaSuccess) return fail(PK_ERR_CUDA, "pk_index_search_noalloc: launch failed");

@@ -17,7 +17,7 @@ namespace {
 using namespace dev;
 
 template <int DT, int KMAX>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, 6)
     search_exact_kernel(const DevGraph *__restrict__ gp, const LaneCfg lc, const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -25,19 +25,15 @@ __global__ void __launch_bounds__(128, 4)
     const int wpb = blockDim.x >> 5;
     const int gwarp = blockIdx.x * wpb + wib;
 
+    const int64_t row_bytes = gp->row_bytes;
     WarpScratch ws;
-    unsigned char *my = smem + (size_t)wib * search_smem_per_warp(a.wcap);
+    unsigned char *my = smem + (size_t)wib * search_smem_per_warp(a.wcap, row_bytes);
     ws.wbuf = reinterpret_cast<Ent *>(my);
     ws.wcap = a.wcap;
     ws.ctop = ws.wbuf + a.wcap;
-    ws.st = reinterpret_cast<Stage *>(ws.ctop + kCandTop);
-    ws.ctail = reinterpret_cast<Ent *>(a.cand_tail) + (size_t)gwarp * a.cand_tail_cap;
-    ws.ccap = kCandTop + a.cand_tail_cap;
-    ws.vis = a.vis + (size_t)gwarp * a.vis_slots;
-    ws.vmask = (uint32_t)a.vis_slots - 1;
-    ws.vshift = 32 - (__ffs(a.vis_slots) - 1);
-    ws.vlimit = (uint32_t)a.vis_slots / 4 * 3;
-    ws.epoch = a.epochs[gwarp];
+    ws.st = reinterpret_cast<Stage *>(my + search_stage_off(a.wcap));
+    ws.rowbuf = reinterpret_cast<uint8_t *>(my + search_rowbuf_off(a.wcap));
+    ws.bind(a.gs, gwarp);
 
     const VecView vv{gp->vec0, gp->zero_row, gp->row_bytes};
     const bool ip = gp->metric == PK_METRIC_IP;
@@ -105,7 +101,6 @@ __global__ void __launch_bounds__(128, 4)
         }
         __syncwarp();
     }
-    if (lane == 0) a.epochs[gwarp] = ws.epoch;
 }
 
 template <int DT>

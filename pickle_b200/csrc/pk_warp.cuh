@@ -200,32 +200,64 @@ __device__ __forceinline__ void dist_rows(const VecView &g, const LaneCfg &lc, c
     }
 }
 
-// ------------------------------------------------------------- visited set --
-// Open addressing over 64-bit slots (epoch << 32 | id): a slot whose epoch is
-// not the current one is empty, so a new layer search only bumps the epoch.
-// The inserting lanes hold distinct ids, so a lost compare-and-swap only means
-// the slot was taken by a neighbour lane.
-// Returns 1 if v was inserted (not visited before), 0 if present, 2 if full.
-__device__ __forceinline__ int vis_insert(unsigned long long *vis, uint32_t mask, int shift, uint32_t epoch,
-                                          int32_t v) {
-    uint32_t h = ((uint32_t)v * 2654435761u) >> shift;
-    const unsigned long long mine = ((unsigned long long)epoch << 32) | (uint32_t)v;
-    for (uint32_t probe = 0; probe <= mask; probe++) {
-        unsigned long long s = vis[h];
-        for (;;) {
-            if ((uint32_t)(s >> 32) != epoch) {
-                const unsigned long long old = atomicCAS(vis + h, s, mine);
-                if (old == s) return 1;
-                s = old;
-                continue;
-            }
-            if ((uint32_t)s == (uint32_t)v) return 0;
-            break;
-        }
-        h = (h + 1) & mask;
-    }
-    return 2;
+// 16-byte asynchronous copy global -> shared (LDGSTS), bypassing L1.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Distances from the query in qr to nrows (<= 32) rows, staged through
+// shared memory kStageRows rows at a time: every lane first issues
+// asynchronous copies of exactly the chunks it will read (its group's rows,
+// its chunk columns), so a batch of rows arrives in one memory round trip;
+// then each group reduces its rows.  rowbuf holds kStageRows rows of
+// row_bytes.  All lanes call it.
+template <int DT, int KMAX>
+__device__ __forceinline__ void dist_rows_staged(const VecView &g, const LaneCfg &lc, const uint4 (&qr)[KMAX],
+                                                 bool ip, const int32_t *rows, float *outd, int nrows,
+                                                 uint8_t *rowbuf, int lane) {
+    typedef Acc<DT> A;
+    const int G = lc.G, R = 32 / G, grp = lane / G, gl = lane % G;
+    const int64_t rb = g.row_bytes;
+    for (int b0 = 0; b0 < nrows; b0 += kStageRows) {
+        const int nb = min(kStageRows, nrows - b0);
+        for (int t = grp; t < nb; t += R) {
+            const uint8_t *src = g.row(rows[b0 + t]);
+            uint8_t *dst = rowbuf + (int64_t)t * rb;
+#pragma unroll
+            for (int k = 0; k < KMAX; k++) {
+                const int c = gl + k * G;
+                if (k < lc.K && c < lc.C) cp_async16(dst + c * 16, src + c * 16);
+            }
+        }
+        cp_async_wait_all();
+        for (int base = 0; base < nb; base += R) {
+            const int t = base + grp;
+            typename A::T acc = 0;
+            if (t < nb) {
+                const uint8_t *row = rowbuf + (int64_t)t * rb;
+#pragma unroll
+                for (int k = 0; k < KMAX; k++) {
+                    const int c = gl + k * G;
+                    if (k < lc.K && c < lc.C) A::add(acc, qr[k], *reinterpret_cast<const uint4 *>(row + c * 16), ip);
+                }
+            }
+            for (int off = G >> 1; off > 0; off >>= 1) acc += A::shfl(acc, off);
+            if (gl == 0 && t < nb) outd[b0 + t] = A::finish(acc, ip);
+        }
+    }
+}
+
+// ------------------------------------------------------------- visited set --
+// An exact visited set per warp: a bitmap over the layer's node ids in global
+// memory.  atomicOr marks a node and tells, in one round trip, whether it was
+// marked before.  The ids marked during a layer search are listed, and the
+// words they touched are zeroed when the search ends, so the next search
+// starts from an empty set without clearing the whole bitmap (a list that
+// overflowed clears the whole bitmap instead).
 
 // ------------------------------------------------------------------- heaps --
 // The reference's EntryHeap: a push moves the new entry up while its parent
@@ -360,25 +392,46 @@ static_assert(sizeof(Stage) == kStageBytes, "staging layout");
 
 // Per-warp working memory of a layer search.
 struct WarpScratch {
-    unsigned long long *vis;  // visited table (global)
-    uint32_t vmask;
-    int vshift;
-    uint32_t vlimit;          // entries allowed before the table counts as full
-    uint32_t epoch;
+    uint32_t *bm;             // visited bitmap (global), bm_words words
+    int64_t bm_words;
+    int32_t *vlist;           // ids marked in the current layer search (global)
+    int vl_cap;
+    int vl_n;
     Ent *wbuf;                // result heap (shared), wcap entries
     int wcap;
     Ent *ctop;                // candidate heap, shared part
     Ent *ctail;               // candidate heap, global part
     int ccap;
     Stage *st;
+    uint8_t *rowbuf;          // shared staging of 32 rows
 
-    __device__ __forceinline__ void next_epoch(int lane) {
-        epoch++;
-        if (epoch == 0) {  // wrapped: clear the table once
-            for (uint32_t i = lane; i <= vmask; i += 32) vis[i] = 0ull;
-            __syncwarp();
-            epoch = 1;
+    __device__ __forceinline__ void bind(const WarpGlobalScratch &g, int64_t gwarp) {
+        bm = g.bitmap + gwarp * g.bm_words;
+        bm_words = g.bm_words;
+        vlist = g.vlist + gwarp * g.vl_cap;
+        vl_cap = g.vl_cap;
+        vl_n = 0;
+        ctail = reinterpret_cast<Ent *>(g.cand_tail) + gwarp * g.cand_tail_cap;
+        ccap = kCandTop + g.cand_tail_cap;
+    }
+
+    // One lane marks v (the entry of a layer search).
+    __device__ __forceinline__ void mark_one(int32_t v) {
+        atomicOr(bm + (v >> 5), 1u << (v & 31));
+        if (vl_n < vl_cap) vlist[vl_n] = v;
+    }
+
+    // End of a layer search: unmark what was marked.  All lanes call it.
+    __device__ __forceinline__ void end_layer(int lane) {
+        __syncwarp();
+        if (vl_n <= vl_cap) {
+            for (int i = lane; i < vl_n; i += 32) bm[vlist[i] >> 5] = 0u;
+        } else {
+            for (int64_t i = lane; i < bm_words; i += 32) bm[i] = 0u;
         }
+        vl_n = 0;
+        __threadfence();
+        __syncwarp();
     }
 };
 
@@ -386,25 +439,29 @@ struct WarpScratch {
 // in range, first within the chunk and not yet visited; mark them; stage ids
 // and vector rows.  Returns the count (warp-uniform).  Ids outside [0, lcap)
 // are skipped (the reference would index its visited table out of range).
+// v_pre: this lane's entry, already loaded (pass have_pre = true).
 __device__ __forceinline__ int take_new(const DevLayer &L, bool layer0, int64_t base, int j0, int deg, WarpScratch &ws,
-                                        int lane, bool &full) {
+                                        int lane, bool have_pre, int32_t v_pre) {
     const int j = j0 + lane;
     int32_t v = -1;
-    if (j < deg) v = L.adj[base + j];
+    if (j < deg) v = have_pre ? v_pre : L.adj[base + j];
     const bool valid = j < deg && v >= 0 && (int64_t)v < L.lcap;
     const int key = valid ? v : -1 - lane;
     const unsigned peers = __match_any_sync(kFull, key);
     const bool first = valid && (__ffs(peers) - 1) == lane;
-    int r = 0;
-    if (first) r = vis_insert(ws.vis, ws.vmask, ws.vshift, ws.epoch, v);
-    const bool is_new = r == 1;
+    bool is_new = false;
+    if (first) {
+        const uint32_t bit = 1u << (v & 31);
+        is_new = (atomicOr(ws.bm + (v >> 5), bit) & bit) == 0;
+    }
     const unsigned nm = __ballot_sync(kFull, is_new);
-    if (__any_sync(kFull, r == 2)) full = true;
     if (is_new) {
         const int pos = __popc(nm & ((1u << lane) - 1));
         ws.st->id[pos] = v;
         ws.st->row[pos] = layer0 ? v : L.vrow[v];
+        if (ws.vl_n + pos < ws.vl_cap) ws.vlist[ws.vl_n + pos] = v;
     }
+    ws.vl_n += __popc(nm);
     __syncwarp();
     return __popc(nm);
 }
@@ -428,24 +485,24 @@ __device__ __forceinline__ float dist_one(const VecView &vv, const LaneCfg &lc, 
 template <int DT, int KMAX, bool COH>
 __device__ int32_t slide_layer(const VecView &vv, const LaneCfg &lc, const uint4 (&qr)[KMAX], bool ip,
                                const DevLayer &L, int32_t enter, WarpScratch &ws, int32_t *cnt, bool &full, int lane) {
-    ws.next_epoch(lane);
     float cd = dist_one<DT, KMAX, COH>(vv, lc, qr, ip, L.vrow[enter], ws, lane);
     int32_t c = enter;
-    uint32_t nvis = 1;
-    if (lane == 0) vis_insert(ws.vis, ws.vmask, ws.vshift, ws.epoch, enter);
+    if (lane == 0) ws.mark_one(enter);
+    ws.vl_n++;
     __syncwarp();
     bool updated;
     int64_t rounds = 0;
     do {
         updated = false;
         const int32_t cur = c;
-        const int deg = L.deg[cur];
         const int64_t base = (int64_t)cur * L.cap;
+        const int32_t pre = lane < L.cap ? L.adj[base + lane] : -1;  // issued with the degree load
+        const int deg = L.deg[cur];
         cnt[0]++;
         cnt[2] += deg;
-        for (int j0 = 0; j0 < deg && !full; j0 += 32) {
-            const int nn = take_new(L, false, base, j0, deg, ws, lane, full);
-            dist_rows<DT, KMAX, COH>(vv, lc, qr, ip, ws.st->row, ws.st->d, nn, lane);
+        for (int j0 = 0; j0 < deg; j0 += 32) {
+            const int nn = take_new(L, false, base, j0, deg, ws, lane, j0 == 0 && L.cap >= 32, pre);
+            dist_rows_staged<DT, KMAX>(vv, lc, qr, ip, ws.st->row, ws.st->d, nn, ws.rowbuf, lane);
             __syncwarp();
             // list order, strict '<': the first occurrence of the minimum wins
             for (int t = 0; t < nn; t++) {
@@ -457,11 +514,11 @@ __device__ int32_t slide_layer(const VecView &vv, const LaneCfg &lc, const uint4
                 }
             }
             cnt[1] += nn;
-            nvis += nn;
-            if (nvis > ws.vlimit) full = true;
             __syncwarp();
         }
-    } while (updated && !full && ++rounds <= L.lcap);
+    } while (updated && ++rounds <= L.lcap);
+    if (rounds > L.lcap) full = true;
+    ws.end_layer(lane);
     return c;
 }
 
@@ -471,7 +528,6 @@ __device__ int32_t slide_layer(const VecView &vv, const LaneCfg &lc, const uint4
 template <int DT, int KMAX, bool COH>
 __device__ int search_layer(const VecView &vv, const LaneCfg &lc, const uint4 (&qr)[KMAX], bool ip, const DevLayer &L,
                             bool layer0, int32_t enter, int ef, WarpScratch &ws, int32_t *cnt, bool &full, int lane) {
-    ws.next_epoch(lane);
     const float ed = dist_one<DT, KMAX, COH>(vv, lc, qr, ip, layer0 ? enter : L.vrow[enter], ws, lane);
     MaxHeap W{ws.wbuf, 0};
     MinHeap C{ws.ctop, ws.ctail, 0, ws.ccap};
@@ -479,10 +535,10 @@ __device__ int search_layer(const VecView &vv, const LaneCfg &lc, const uint4 (&
         const Ent e{ed, enter};
         W.push(e);
         C.push(e);
-        vis_insert(ws.vis, ws.vmask, ws.vshift, ws.epoch, enter);
+        ws.mark_one(enter);
     }
+    ws.vl_n++;
     __syncwarp();
-    uint32_t nvis = 1;
     int64_t hops = 0;
     for (;;) {
         int32_t cid = -1;
@@ -492,13 +548,14 @@ __device__ int search_layer(const VecView &vv, const LaneCfg &lc, const uint4 (&
         }
         cid = __shfl_sync(kFull, cid, 0);
         if (cid < 0) break;
-        const int deg = L.deg[cid];
         const int64_t base = (int64_t)cid * L.cap;
+        const int32_t pre = lane < L.cap ? L.adj[base + lane] : -1;  // issued with the degree load
+        const int deg = L.deg[cid];
         cnt[0]++;
         cnt[2] += deg;
         for (int j0 = 0; j0 < deg && !full; j0 += 32) {
-            const int nn = take_new(L, layer0, base, j0, deg, ws, lane, full);
-            dist_rows<DT, KMAX, COH>(vv, lc, qr, ip, ws.st->row, ws.st->d, nn, lane);
+            const int nn = take_new(L, layer0, base, j0, deg, ws, lane, j0 == 0 && L.cap >= 32, pre);
+            dist_rows_staged<DT, KMAX>(vv, lc, qr, ip, ws.st->row, ws.st->d, nn, ws.rowbuf, lane);
             __syncwarp();
             int over = 0;
             if (lane == 0) {
@@ -518,8 +575,6 @@ __device__ int search_layer(const VecView &vv, const LaneCfg &lc, const uint4 (&
             }
             if (__shfl_sync(kFull, over, 0)) full = true;
             cnt[1] += nn;
-            nvis += nn;
-            if (nvis > ws.vlimit) full = true;
             __syncwarp();
         }
         if (full || ++hops > L.lcap) {
@@ -527,6 +582,7 @@ __device__ int search_layer(const VecView &vv, const LaneCfg &lc, const uint4 (&
             break;
         }
     }
+    ws.end_layer(lane);
     int wl = W.len;
     wl = __shfl_sync(kFull, wl, 0);
     return wl;

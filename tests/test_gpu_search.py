@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
-@pytest.mark.parametrize("ef", [10, 48])
+@pytest.mark.parametrize("ef", [10, 33, 48])
 def test_search_matches_oracle(name, ef, gpu, ref_bin):
     metric, base, queries, M, efc = case_data(name)
     path = ref_graph(name)
