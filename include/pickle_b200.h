@@ -114,6 +114,72 @@ int pk_index_search_device(pk_index *h, const void *queries, int64_t nq, int32_t
                            const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride,
                            int32_t *out_ids, float *out_dists, int32_t *counters, void *stream);
 
+/* Traversal precisions of the batched low-precision search. */
+#define PK_TRAVERSAL_F16 1   /* FP16 copy of the vectors */
+#define PK_TRAVERSAL_FP8 2   /* FP8 E4M3 copy, scaled per dimension */
+
+/* Builds the low-precision copy of the vectors that pk_index_search_fast
+ * walks the graph with (FP16, or FP8 E4M3 with one scale per dimension taken
+ * from the rows present now; rows inserted later reuse those scales).
+ * Synchronous.  Extends the reference, which walks with the original vectors
+ * only (include/hnsw.hpp:373-444). */
+int pk_index_prepare_fast(pk_index *h, int traversal);
+
+/* Batched search that walks the graph with the low-precision copy and
+ * re-ranks the ef listed candidates with exact distances from the original
+ * vectors (the returned distances are exact; the ids may differ from the
+ * exact search's where low-precision distances reorder the walk).  Arguments
+ * as pk_index_search_device; `ef` bounds ef_per_query; expand = list entries
+ * expanded per step (1..4, 0 = 1).  Fully asynchronous on `stream` (no host
+ * synchronisation), so it can be captured in a CUDA graph once buffers have
+ * grown to the batch size by an earlier call.  Successive calls on one
+ * handle share its scratch: order them on one stream. */
+int pk_index_search_fast(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                         const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride,
+                         int32_t *out_ids, float *out_dists, int32_t *counters, int32_t expand, void *stream);
+
+/* pk_index_search_fast with host buffers (queries nq*dim in, out_ids /
+ * out_dists nq*k out); synchronous. */
+int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
+                              float *out_dists, int32_t expand);
+
+/* Serving: continuous batching over pk_index_search_fast.  No counterpart
+ * in the reference (its batch AnnSearch is a blocking OpenMP loop,
+ * include/hnsw.hpp:528-541).  A worker thread owns `slots` execution slots,
+ * each with its own stream, scratch and buffers for max_batch queries
+ * (allocated at creation: device memory is fixed, admission is by slot and
+ * batch capacity).  Submitted requests (nq queries sharing one k <= max_k and
+ * one ef <= max_ef) wait in FIFO order and are packed into whichever slot frees
+ * up first; slots in flight overlap on the GPU.  Each result equals what
+ * pk_index_search_fast returns for that request alone.  A slot that does not
+ * finish within the watchdog period (30 s) fails its requests with
+ * PK_ERR_TIMEOUT.  The index must not be modified while a server uses it.
+ * submit copies the queries and returns a ticket at once; wait blocks until
+ * the ticket's results are ready (timeout_ms < 0: no limit), copies nq*k ids
+ * and distances out, and reports the latency from submit to completion.
+ * stats: out[0..4] = batches launched, queries served, most slots in flight
+ * at once, requests queued, error status. */
+typedef struct pk_server pk_server;
+int pk_server_create(pk_server **out, pk_index *h, int traversal, int slots, int32_t max_batch, int32_t max_k,
+                     int32_t max_ef, int32_t expand);
+int pk_server_submit(pk_server *s, const void *queries, int32_t nq, int32_t k, int32_t ef, int64_t *ticket);
+int pk_server_wait(pk_server *s, int64_t ticket, int32_t *out_ids, float *out_dists, double *latency_ms,
+                   int32_t timeout_ms);
+int pk_server_stats(pk_server *s, int64_t *out);
+/* Replays a timed request trace through the server: request i (nq[i]
+ * consecutive rows of `queries`, k[i], ef[i]) is submitted arrival_us[i]
+ * microseconds after the call starts, by a producer thread that waits for each
+ * arrival time; results land in out_ids / out_dists (rows of out_stride, may
+ * be NULL) and each request's submit-to-completion latency in latency_ms[i].
+ * For measuring latency under a given arrival process (e.g. Poisson). */
+int pk_server_replay(pk_server *s, const void *queries, int64_t n, const int32_t *nq, const double *arrival_us,
+                     const int32_t *k, const int32_t *ef, int32_t *out_ids, float *out_dists, int32_t out_stride,
+                     double *latency_ms);
+/* Watchdog period in seconds (default 30): how long a slot may stay in flight
+ * before its requests fail with PK_ERR_TIMEOUT. */
+int pk_server_set_watchdog(pk_server *s, double seconds);
+int pk_server_destroy(pk_server *s);
+
 /* No counterpart in the reference.  The exact device search of
  * pk_index_search_device (uniform k and ef, device pointers, asynchronous work
  * on `stream` but the call waits for it) without any device allocation: for

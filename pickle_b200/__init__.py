@@ -17,7 +17,7 @@ import os
 
 import numpy as np
 
-__all__ = ["HNSWIndex", "PickleError", "lib", "DTYPES", "METRICS", "LIB_PATH"]
+__all__ = ["HNSWIndex", "Server", "PickleError", "lib", "DTYPES", "METRICS", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpickle_b200.so")
@@ -66,9 +66,23 @@ def lib() -> ctypes.CDLL:
         L.pk_index_load.argtypes = [PP, ctypes.c_char_p]
         L.pk_index_info.argtypes = [P, VP]
         L.pk_index_layer.argtypes = [P, ctypes.c_int] + [VP] * 3 + [VP] * 6
+        L.pk_index_prepare_fast.argtypes = [P, ctypes.c_int]
+        L.pk_index_search_fast.argtypes = [P, VP, I64, I32, I32, VP, VP, I32, VP, VP, VP, I32, VP]
+        L.pk_index_search_fast_host.argtypes = [P, VP, I64, I32, I32, VP, VP, I32]
+        L.pk_index_search_noalloc.argtypes = [P, VP, I64, I32, I32, VP, VP, VP]
+        L.pk_server_create.argtypes = [PP, P, ctypes.c_int, ctypes.c_int, I32, I32, I32, I32]
+        L.pk_server_submit.argtypes = [P, VP, I32, I32, I32, ctypes.POINTER(ctypes.c_int64)]
+        L.pk_server_wait.argtypes = [P, ctypes.c_int64, VP, VP, ctypes.POINTER(ctypes.c_double), I32]
+        L.pk_server_stats.argtypes = [P, VP]
+        L.pk_server_set_watchdog.argtypes = [P, ctypes.c_double]
+        L.pk_server_destroy.argtypes = [P]
+        L.pk_server_replay.argtypes = [P, VP, I64, VP, VP, VP, VP, VP, VP, I32, VP]
         for name in ["pk_index_create", "pk_index_destroy", "pk_index_set_seed", "pk_index_set_levels",
                      "pk_index_build", "pk_index_add", "pk_index_search", "pk_index_search_device",
-                     "pk_index_save", "pk_index_load", "pk_index_info", "pk_index_layer"]:
+                     "pk_index_save", "pk_index_load", "pk_index_info", "pk_index_layer", "pk_index_prepare_fast",
+                     "pk_index_search_fast", "pk_index_search_fast_host", "pk_index_search_noalloc",
+                     "pk_server_create", "pk_server_submit", "pk_server_wait", "pk_server_stats",
+                     "pk_server_set_watchdog", "pk_server_destroy", "pk_server_replay"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -166,6 +180,31 @@ class HNSWIndex:
                                             _dev_ptr(ef_per_query), stride, _dev_ptr(out_ids), _dev_ptr(out_dists),
                                             _dev_ptr(counters), s))
 
+    # ---- batched low-precision search ----------------------------------
+    TRAVERSAL = {"f16": 1, "fp8": 2}
+
+    def prepare_fast(self, traversal: str = "fp8") -> None:
+        """Build the FP16 / FP8 (per-dimension scaled) copy the fast search walks with."""
+        _check(lib().pk_index_prepare_fast(self._h, self.TRAVERSAL[traversal]))
+
+    def search_fast_device(self, queries, k: int, ef: int, out_ids, out_dists, k_per_query=None, ef_per_query=None,
+                           counters=None, expand: int = 1, stream=None) -> None:
+        """Low-precision walk + exact re-rank on torch CUDA tensors (asynchronous)."""
+        nq = queries.shape[0]
+        s = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _check(lib().pk_index_search_fast(self._h, _dev_ptr(queries), nq, k, ef, _dev_ptr(k_per_query),
+                                          _dev_ptr(ef_per_query), out_ids.shape[1], _dev_ptr(out_ids),
+                                          _dev_ptr(out_dists), _dev_ptr(counters), expand, s))
+
+    def search_fast(self, queries: np.ndarray, k: int, ef: int, expand: int = 1):
+        """Low-precision walk + exact re-rank with host buffers: (ids, dists)."""
+        q = self._rows(queries)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.int32)
+        dists = np.empty((nq, k), np.float32)
+        _check(lib().pk_index_search_fast_host(self._h, _ptr(q), nq, k, ef, _ptr(ids), _ptr(dists), expand))
+        return ids, dists
+
     # ---- persistence ----------------------------------------------------
     def save(self, path: str) -> None:
         _check(lib().pk_index_save(self._h, os.fsencode(path)))
@@ -208,3 +247,69 @@ class HNSWIndex:
         if a.dtype != self.dtype:
             raise TypeError(f"expected {self.dtype}, got {a.dtype}")
         return a
+
+
+class Server:
+    """Continuous-batching search server over an index (pk_server_* in the C ABI).
+
+    Server(index, traversal="f16", slots=4, max_batch=4096, max_k=100, max_ef=256)
+    submit(queries, k, ef) -> ticket (returns at once); wait(ticket) -> (ids, dists, latency_ms).
+    """
+
+    def __init__(self, index: "HNSWIndex", traversal: str = "f16", slots: int = 4, max_batch: int = 4096,
+                 max_k: int = 100, max_ef: int = 256, expand: int = 1):
+        self.index = index
+        self._s = None
+        s = ctypes.c_void_p()
+        _check(lib().pk_server_create(ctypes.byref(s), index._h, HNSWIndex.TRAVERSAL[traversal], slots, max_batch,
+                                      max_k, max_ef, expand))
+        self._s = s
+        self._shape = {}
+
+    def submit(self, queries: np.ndarray, k: int, ef: int) -> int:
+        q = self.index._rows(queries)
+        t = ctypes.c_int64()
+        _check(lib().pk_server_submit(self._s, _ptr(q), q.shape[0], k, ef, ctypes.byref(t)))
+        self._shape[t.value] = (q.shape[0], k)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        nq, k = self._shape.pop(ticket)
+        ids = np.empty((nq, k), np.int32)
+        dists = np.empty((nq, k), np.float32)
+        lat = ctypes.c_double()
+        _check(lib().pk_server_wait(self._s, ticket, _ptr(ids), _ptr(dists), ctypes.byref(lat), timeout_ms))
+        return ids, dists, lat.value
+
+    def replay(self, queries: np.ndarray, nq: np.ndarray, arrival_us: np.ndarray, k: np.ndarray, ef: np.ndarray,
+               out_stride: int = 0):
+        """Replay a timed trace natively; returns (ids, dists, latency_ms per request)."""
+        q = self.index._rows(queries)
+        nq = np.ascontiguousarray(nq, np.int32)
+        arr = np.ascontiguousarray(arrival_us, np.float64)
+        k = np.ascontiguousarray(k, np.int32)
+        ef = np.ascontiguousarray(ef, np.int32)
+        n = len(nq)
+        stride = out_stride or int(k.max())
+        ids = np.full((int(nq.sum()), stride), -1, np.int32)
+        dists = np.full((int(nq.sum()), stride), np.inf, np.float32)
+        lat = np.zeros(n, np.float64)
+        _check(lib().pk_server_replay(self._s, _ptr(q), n, _ptr(nq), _ptr(arr), _ptr(k), _ptr(ef), _ptr(ids),
+                                      _ptr(dists), stride, _ptr(lat)))
+        return ids, dists, lat
+
+    def set_watchdog(self, seconds: float) -> None:
+        _check(lib().pk_server_set_watchdog(self._s, seconds))
+
+    def stats(self) -> dict:
+        out = np.zeros(5, np.int64)
+        _check(lib().pk_server_stats(self._s, _ptr(out)))
+        return dict(zip(["batches", "queries", "max_inflight", "queued", "error"], (int(x) for x in out)))
+
+    def close(self) -> None:
+        if getattr(self, "_s", None):
+            lib().pk_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        self.close()

@@ -60,6 +60,15 @@ def cmd_search(a):
     dev = torch.device("cuda")
     qd = torch.from_numpy(q).to(dev)
     nq = len(q)
+    if a.path != "exact":
+        idx.prepare_fast(a.path)
+
+    def run(k, ef, ids, ds, counters=None):
+        if a.path == "exact":
+            idx.search_device(qd, k, ef, ids, ds, counters=counters)
+        else:
+            idx.search_fast_device(qd, k, ef, ids, ds, counters=counters, expand=a.expand)
+
     for k in ks:
         for ef in efs:
             if ef < k:
@@ -70,13 +79,13 @@ def cmd_search(a):
             for _ in range(max(1, a.repeat)):
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
-                idx.search_device(qd, k, ef, ids, ds)
+                run(k, ef, ids, ds)
                 torch.cuda.synchronize()
                 times.append(time.perf_counter() - t0)
             secs = sorted(times)[len(times) // 2]
             cnt = torch.zeros((nq, 6), dtype=torch.int32, device=dev)
             if not a.no_metrics:
-                idx.search_device(qd, k, ef, ids, ds, counters=cnt)
+                run(k, ef, ids, ds, counters=cnt)
                 torch.cuda.synchronize()
             c = cnt.double().sum(0).cpu().numpy() / nq
             recall = 100.0 * datasets.recall_at_k(ids.cpu().numpy(), labels, k) if labels is not None else float("nan")
@@ -140,6 +149,9 @@ def main(argv=None):
     s.add_argument("--ef", type=int, default=0)
     s.add_argument("--repeat", type=int, default=3)
     s.add_argument("--no_metrics", action="store_true")
+    s.add_argument("--path", default="exact", choices=["exact", "f16", "fp8"],
+                   help="exact: the reference's search; f16/fp8: low-precision walk + exact re-rank")
+    s.add_argument("--expand", type=int, default=1)
     g = sub.add_parser("gen")
     g.add_argument("--config", required=True)
     g.add_argument("--out", required=True)

@@ -11,6 +11,12 @@
 //             down, replacing the reference's ext2in lookups);
 //   a DevGraph block holding all of the above, read by the kernels.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -23,6 +29,7 @@
 #include <vector>
 
 #include "pk_build.h"
+#include "pk_fast.h"
 #include "pk_format.h"
 #include "pk_internal.h"
 
@@ -100,6 +107,16 @@ struct SearchScratch {
     }
 };
 
+// Per-launch working set of the fast search: scratch and query staging.  The
+// handle owns one; each serving slot owns its own, so slots can overlap.
+struct FastCtx {
+    SearchScratch fs;
+    uint8_t *d_fq = nullptr, *d_tq = nullptr;
+    int64_t fq_n = 0, tq_n = 0;
+    float *d_qn = nullptr;
+    int64_t qn_n = 0;
+};
+
 }  // namespace
 
 struct pk_index {
@@ -135,6 +152,16 @@ struct pk_index {
     int64_t status_n = 0;
     int32_t *d_qlist = nullptr;
     int64_t qlist_n = 0;
+
+    // low-precision traversal copy and the fast path's scratch
+    int trav = 0;                  // 0 none, pk::kTravF16, pk::kTravE4M3
+    int64_t trav_row_bytes = 0, trav_rows = 0, trav_cap = 0;
+    uint8_t *d_trav = nullptr, *d_trav_zero = nullptr;
+    float *d_scale = nullptr, *d_rownorm = nullptr;
+    FastCtx fctx;
+    int32_t *d_fids = nullptr;
+    float *d_fdists = nullptr;
+    int64_t fids_n = 0, fdists_n = 0;
 
     size_t dev_bytes = 0;
 
@@ -671,6 +698,128 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
     return PK_OK;
 }
 
+// ------------------------------------------------------------ fast path -----
+
+// (Re)builds the traversal copy of rows [0, n0): per-dimension scales from
+// the rows present now (FP8), then every row converted.
+int build_traversal(pk_index *h, int trav) {
+    cudaStream_t s = h->stream;
+    const int64_t trb = trav == pk::kTravF16 ? pk::align16(h->dim * 2) : pk::align16(h->dim);
+    const int64_t rows = std::max<int64_t>(h->vec_rows, 1);
+    PK_CUDA(cudaStreamSynchronize(s));
+    dfree(h, h->d_trav, (size_t)(h->trav_cap * h->trav_row_bytes));
+    dfree(h, h->d_rownorm, 4 * (size_t)h->trav_cap);
+    dfree(h, h->d_trav_zero, (size_t)h->trav_row_bytes);
+    dfree(h, h->d_scale, 4 * (size_t)h->dim);
+    h->d_trav = nullptr;
+    h->trav = 0;
+    PK_TRY(dalloc(h, (void **)&h->d_trav, (size_t)(rows * trb)));
+    PK_TRY(dalloc(h, (void **)&h->d_rownorm, 4 * (size_t)rows));
+    PK_TRY(dalloc(h, (void **)&h->d_trav_zero, (size_t)trb));
+    PK_TRY(dalloc(h, (void **)&h->d_scale, 4 * (size_t)h->dim));
+    PK_CUDA(cudaMemsetAsync(h->d_trav, 0, (size_t)(rows * trb), s));
+    PK_CUDA(cudaMemsetAsync(h->d_trav_zero, 0, (size_t)trb, s));
+    PK_CUDA(cudaMemsetAsync(h->d_rownorm, 0, 4 * (size_t)rows, s));
+    std::vector<float> scale(h->dim, 1.0f);
+    if (trav == pk::kTravE4M3 && h->n0() > 0) {
+        uint32_t *amax = nullptr;
+        PK_TRY(dalloc(h, (void **)&amax, 4 * (size_t)h->dim));
+        PK_CUDA(cudaMemsetAsync(amax, 0, 4 * (size_t)h->dim, s));
+        PK_CUDA(pk::launch_absmax(h->dtype, h->hg.vec0, h->row_bytes, h->n0(), (int)h->dim, amax, s));
+        std::vector<float> m(h->dim);
+        PK_CUDA(cudaMemcpyAsync(m.data(), amax, 4 * (size_t)h->dim, cudaMemcpyDeviceToHost, s));
+        PK_CUDA(cudaStreamSynchronize(s));
+        dfree(h, amax, 4 * (size_t)h->dim);
+        // E4M3's largest finite value is 448: map each dimension's largest
+        // magnitude onto it
+        for (int64_t d = 0; d < h->dim; d++) scale[d] = m[d] > 0.f ? m[d] / 448.0f : 1.0f;
+    }
+    PK_CUDA(cudaMemcpyAsync(h->d_scale, scale.data(), 4 * (size_t)h->dim, cudaMemcpyHostToDevice, s));
+    PK_CUDA(pk::launch_convert_rows(h->dtype, trav, h->hg.vec0, h->row_bytes, 0, h->n0(), (int)h->dim, h->d_scale,
+                                    h->d_trav, trb, h->d_rownorm, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    h->trav = trav;
+    h->trav_row_bytes = trb;
+    h->trav_rows = h->n0();
+    h->trav_cap = rows;
+    return PK_OK;
+}
+
+// Rows inserted since the copy was built are converted with the same scales.
+int refresh_traversal(pk_index *h) {
+    if (h->trav_rows == h->n0()) return PK_OK;
+    if (h->vec_rows > h->trav_cap) return build_traversal(h, h->trav);
+    PK_CUDA(pk::launch_convert_rows(h->dtype, h->trav, h->hg.vec0, h->row_bytes, h->trav_rows, h->n0(), (int)h->dim,
+                                    h->d_scale, h->d_trav, h->trav_row_bytes, h->d_rownorm, h->stream));
+    PK_CUDA(cudaStreamSynchronize(h->stream));
+    h->trav_rows = h->n0();
+    return PK_OK;
+}
+
+int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_queries, int64_t nq, int32_t k,
+                    int32_t ef, const int32_t *k_arr, const int32_t *ef_arr, int32_t stride, int32_t *ids,
+                    float *dists, int32_t *counters, int32_t expand, cudaStream_t s) {
+    if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
+    PK_TRY(refresh_traversal(h));
+    const int list_cap = (int)pow2ceil(std::max(32, ef));
+    if (list_cap > 4096) return fail(PK_ERR_ARG, "ef too large for the fast path (max 4096)");
+    const int rowbuf = (int)(pk::kStageRows * std::max(h->row_bytes, h->trav_row_bytes));
+    int wpb = 4;
+    size_t smem = (size_t)wpb * pk::fast_smem_per_warp(list_cap, rowbuf);
+    while (wpb > 1 && smem > 200 * 1024) {
+        wpb /= 2;
+        smem = (size_t)wpb * pk::fast_smem_per_warp(list_cap, rowbuf);
+    }
+    const pk::TravCfgHost tc = pk::trav_config(h->trav_row_bytes, h->trav);
+    const int nb = pk::fast_blocks_per_sm(h->dtype, h->lc, h->trav, tc, wpb, smem);
+    if (nb <= 0) return fail(PK_ERR_CUDA, "fast search kernel cannot be resident");
+    const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + wpb - 1) / wpb);
+    const int64_t bm_words = (h->hg.L[0].lcap + 31) / 32 + 1;
+    PK_TRY(ensure_scratch(h, c.fs, grid * wpb, bm_words, std::max<int64_t>(8192, 64LL * ef), 1));
+    // exact queries (padded rows) and traversal queries
+    const size_t w = (size_t)(h->dim * h->esz);
+    const uint8_t *qx = static_cast<const uint8_t *>(queries);
+    if (host_queries || w != (size_t)h->row_bytes || ((uintptr_t)queries & 15) != 0) {
+        PK_TRY(ensure_buf(h, &c.d_fq, c.fq_n, nq * h->row_bytes));
+        if (w != (size_t)h->row_bytes) PK_CUDA(cudaMemsetAsync(c.d_fq, 0, (size_t)(nq * h->row_bytes), s));
+        PK_CUDA(cudaMemcpy2DAsync(c.d_fq, (size_t)h->row_bytes, queries, w, w, (size_t)nq,
+                                  host_queries ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+        qx = c.d_fq;
+    }
+    const int64_t tq_rb = h->trav == pk::kTravF16 ? h->trav_row_bytes : (h->trav_row_bytes / 16) * 64;
+    PK_TRY(ensure_buf(h, &c.d_tq, c.tq_n, nq * tq_rb));
+    PK_TRY(ensure_buf(h, &c.d_qn, c.qn_n, nq));
+    PK_CUDA(pk::launch_prep_queries(h->dtype, h->trav, qx, h->row_bytes, nq, (int)h->dim, h->d_scale, c.d_tq, tq_rb,
+                                    c.d_qn, s));
+    PK_CUDA(cudaMemsetAsync(c.fs.work, 0, sizeof(int32_t) * 2, s));
+    pk::FastArgs a{};
+    a.nq = nq;
+    a.k = k;
+    a.ef = ef;
+    a.k_arr = k_arr;
+    a.ef_arr = ef_arr;
+    a.out_stride = stride;
+    a.out_ids = ids;
+    a.out_dists = dists;
+    a.ext0 = h->hg.L[0].ext;
+    a.counters = counters;
+    a.work = c.fs.work;
+    a.gs = c.fs.view();
+    a.list_cap = list_cap;
+    a.rowbuf_bytes = rowbuf;
+    a.expand = std::max(1, std::min(4, expand > 0 ? expand : 1));
+    a.queries = qx;
+    a.tq_rows = c.d_tq;
+    a.tq_row_bytes = tq_rb;
+    a.qnorm = c.d_qn;
+    a.trav = h->d_trav;
+    a.trav_zero = h->d_trav_zero;
+    a.trav_row_bytes = h->trav_row_bytes;
+    a.rownorm = h->d_rownorm;
+    PK_CUDA(pk::launch_search_fast(h->dg, h->dtype, h->lc, h->trav, tc, a, (int)grid, wpb, smem, s));
+    return PK_OK;
+}
+
 // --------------------------------------------------------------- create -----
 
 int init_handle(pk_index *h, int metric, int dtype, int64_t dim, int64_t M, int64_t efc) {
@@ -712,6 +861,14 @@ int init_handle(pk_index *h, int metric, int dtype, int64_t dim, int64_t M, int6
     return PK_OK;
 }
 
+void free_fast_ctx(pk_index *h, FastCtx &c) {
+    free_scratch(h, c.fs);
+    dfree(h, c.d_fq, (size_t)c.fq_n);
+    dfree(h, c.d_tq, (size_t)c.tq_n);
+    dfree(h, c.d_qn, 4 * (size_t)c.qn_n);
+    c = FastCtx{};
+}
+
 void destroy_handle(pk_index *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
@@ -734,6 +891,13 @@ void destroy_handle(pk_index *h) {
         cudaFree(s->cand_tail);
         cudaFree(s->work);
     }
+    cudaFree(h->d_trav);
+    cudaFree(h->d_trav_zero);
+    cudaFree(h->d_scale);
+    cudaFree(h->d_rownorm);
+    free_fast_ctx(h, h->fctx);
+    cudaFree(h->d_fids);
+    cudaFree(h->d_fdists);
     cudaFree(h->d_qstage);
     cudaFree(h->d_ids);
     cudaFree(h->d_dists);
@@ -1052,6 +1216,388 @@ static int pk_index_layer_impl(const pk_index *hc, int level, int64_t *n, int64_
 
 }  // namespace
 
+namespace {
+
+static int pk_index_prepare_fast_impl(pk_index *h, int traversal) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    if (traversal != PK_TRAVERSAL_F16 && traversal != PK_TRAVERSAL_FP8)
+        return fail(PK_ERR_ARG, "traversal must be PK_TRAVERSAL_F16 or PK_TRAVERSAL_FP8");
+    return build_traversal(h, traversal == PK_TRAVERSAL_F16 ? pk::kTravF16 : pk::kTravE4M3);
+}
+
+static int pk_index_search_fast_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                                     const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride,
+                                     int32_t *out_ids, float *out_dists, int32_t *counters, int32_t expand,
+                                     void *stream) {
+    if (!h || nq < 0 || ((!queries || !out_ids || !out_dists) && nq > 0)) return fail(PK_ERR_ARG, "bad arguments");
+    if (k < 1 || ef < 1 || out_stride < k) return fail(PK_ERR_ARG, "need k >= 1, ef >= 1, out_stride >= k");
+    if (nq == 0) return PK_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (h->n0() == 0) {
+        PK_CUDA(fill_i32(out_ids, nq * out_stride, -1, s));
+        PK_CUDA(fill_f32(out_dists, nq * out_stride, FLT_MAX, s));
+        return PK_OK;
+    }
+    return run_search_fast(h, h->fctx, queries, false, nq, k, ef, k_per_query, ef_per_query, out_stride, out_ids,
+                           out_dists, counters, expand, s);
+}
+
+static int pk_index_search_fast_host_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                                          int32_t *out_ids, float *out_dists, int32_t expand) {
+    if (!h || nq < 0 || ((!queries || !out_ids || !out_dists) && nq > 0)) return fail(PK_ERR_ARG, "bad arguments");
+    if (k < 1 || ef < 1) return fail(PK_ERR_ARG, "k and ef must be >= 1");
+    if (nq == 0) return PK_OK;
+    if (h->n0() == 0) {
+        for (int64_t i = 0; i < nq * k; i++) {
+            out_ids[i] = -1;
+            out_dists[i] = FLT_MAX;
+        }
+        return PK_OK;
+    }
+    cudaStream_t s = h->stream;
+    PK_TRY(ensure_buf(h, &h->d_fids, h->fids_n, nq * k));
+    PK_TRY(ensure_buf(h, &h->d_fdists, h->fdists_n, nq * k));
+    PK_TRY(run_search_fast(h, h->fctx, queries, true, nq, k, ef, nullptr, nullptr, k, h->d_fids, h->d_fdists,
+                           nullptr, expand, s));
+    PK_CUDA(cudaMemcpyAsync(out_ids, h->d_fids, sizeof(int32_t) * nq * k, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaMemcpyAsync(out_dists, h->d_fdists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    return PK_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- server ----
+// Continuous batching over the fast search.  A worker thread owns `slots`
+// execution slots; each has its own stream, scratch (FastCtx), pinned host
+// staging and device buffers sized for max_batch queries.  Requests (each a
+// group of queries with one k and ef) wait in a FIFO; whenever a slot is free,
+// the worker packs queued requests into it up to max_batch queries, copies
+// them in, launches the search with per-query k and ef, copies the results
+// out and records an event.  Slots in flight overlap on the device; a slot is
+// refilled as soon as its event completes.  Device memory is fixed at creation
+// (admission is by slot and batch capacity); a slot whose work has not
+// completed within the watchdog period fails its requests with
+// PK_ERR_TIMEOUT.
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct SrvRequest {
+    int64_t ticket = 0;
+    int32_t nq = 0, k = 0, ef = 0;
+    std::vector<uint8_t> q;
+    std::vector<int32_t> ids;
+    std::vector<float> dists;
+    Clock::time_point t_submit, t_done;
+    int status = 0;
+    bool done = false;
+};
+
+struct SrvSlot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    FastCtx ctx;
+    uint8_t *h_q = nullptr;
+    int32_t *h_k = nullptr, *h_ef = nullptr, *h_ids = nullptr;
+    float *h_d = nullptr;
+    uint8_t *d_q = nullptr;
+    int32_t *d_k = nullptr, *d_ef = nullptr, *d_ids = nullptr;
+    float *d_d = nullptr;
+    bool busy = false;
+    std::vector<std::shared_ptr<SrvRequest>> reqs;
+    std::vector<int32_t> offs;
+    int32_t nq = 0;
+    Clock::time_point t_launch;
+};
+
+}  // namespace
+
+struct pk_server {
+    pk_index *h = nullptr;
+    int32_t max_batch = 0, max_k = 0, max_ef = 0, expand = 1;
+    double watchdog_s = 30.0;
+    std::vector<SrvSlot> slots;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<SrvRequest>> queue;
+    std::unordered_map<int64_t, std::shared_ptr<SrvRequest>> table;
+    int64_t next_ticket = 1;
+    bool stop = false;
+    int error = 0;
+    std::thread worker;
+    // statistics
+    int64_t batches = 0, queries = 0, max_inflight = 0;
+};
+
+namespace {
+
+void srv_fail_all(pk_server *S, int code) {
+    // caller holds S->mu
+    S->error = code;
+    for (auto &kv : S->table)
+        if (!kv.second->done) {
+            kv.second->status = code;
+            kv.second->done = true;
+            kv.second->t_done = Clock::now();
+        }
+    S->cv_done.notify_all();
+}
+
+void srv_loop(pk_server *S) {
+    pk_index *h = S->h;
+    cudaSetDevice(h->device);
+    const size_t w = (size_t)(h->dim * h->esz);
+    for (;;) {
+        bool did = false;
+        // 1. completions
+        for (SrvSlot &sl : S->slots) {
+            if (!sl.busy) continue;
+            // the watchdog looks first: a slot whose completion the host has
+            // not observed within the period fails, finished or not
+            double wd;
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                wd = S->watchdog_s;
+            }
+            if (std::chrono::duration<double>(Clock::now() - sl.t_launch).count() > wd) {
+                std::lock_guard<std::mutex> lk(S->mu);
+                for (auto &r : sl.reqs) {
+                    r->status = PK_ERR_TIMEOUT;
+                    r->done = true;
+                    r->t_done = Clock::now();
+                }
+                sl.reqs.clear();
+                sl.offs.clear();
+                srv_fail_all(S, PK_ERR_TIMEOUT);
+                sl.busy = false;
+                continue;
+            }
+            const cudaError_t e = cudaEventQuery(sl.ev);
+            if (e == cudaErrorNotReady) continue;
+            const auto now = Clock::now();
+            std::lock_guard<std::mutex> lk(S->mu);
+            for (size_t i = 0; i < sl.reqs.size(); i++) {
+                SrvRequest &r = *sl.reqs[i];
+                if (e != cudaSuccess) {
+                    r.status = PK_ERR_CUDA;
+                } else {
+                    r.ids.resize((size_t)r.nq * r.k);
+                    r.dists.resize((size_t)r.nq * r.k);
+                    for (int32_t j = 0; j < r.nq; j++) {
+                        const int64_t row = sl.offs[i] + j;
+                        std::memcpy(r.ids.data() + (size_t)j * r.k, sl.h_ids + row * S->max_k, 4 * (size_t)r.k);
+                        std::memcpy(r.dists.data() + (size_t)j * r.k, sl.h_d + row * S->max_k, 4 * (size_t)r.k);
+                    }
+                }
+                r.done = true;
+                r.t_done = now;
+            }
+            if (e != cudaSuccess) srv_fail_all(S, PK_ERR_CUDA);
+            sl.reqs.clear();
+            sl.offs.clear();
+            sl.busy = false;
+            did = true;
+            S->cv_done.notify_all();
+        }
+        // 2. admissions into free slots
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            if (S->stop) break;
+            int inflight = 0;
+            for (SrvSlot &sl : S->slots) inflight += sl.busy;
+            for (SrvSlot &sl : S->slots) {
+                if (sl.busy || S->queue.empty() || S->error) continue;
+                int32_t nq = 0;
+                while (!S->queue.empty() && nq + S->queue.front()->nq <= S->max_batch) {
+                    auto r = S->queue.front();
+                    S->queue.pop_front();
+                    sl.offs.push_back(nq);
+                    std::memcpy(sl.h_q + (size_t)nq * w, r->q.data(), (size_t)r->nq * w);
+                    for (int32_t j = 0; j < r->nq; j++) {
+                        sl.h_k[nq + j] = r->k;
+                        sl.h_ef[nq + j] = r->ef;
+                    }
+                    nq += r->nq;
+                    sl.reqs.push_back(std::move(r));
+                }
+                if (nq == 0) continue;
+                sl.nq = nq;
+                lk.unlock();
+                int rc = PK_OK;
+                if (cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)nq * w, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
+                    cudaMemcpyAsync(sl.d_k, sl.h_k, 4 * (size_t)nq, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
+                    cudaMemcpyAsync(sl.d_ef, sl.h_ef, 4 * (size_t)nq, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess)
+                    rc = PK_ERR_CUDA;
+                if (rc == PK_OK)
+                    rc = run_search_fast(h, sl.ctx, sl.d_q, false, nq, S->max_k, S->max_ef, sl.d_k, sl.d_ef, S->max_k,
+                                         sl.d_ids, sl.d_d, nullptr, S->expand, sl.stream);
+                if (rc == PK_OK &&
+                    (cudaMemcpyAsync(sl.h_ids, sl.d_ids, 4 * (size_t)nq * S->max_k, cudaMemcpyDeviceToHost,
+                                     sl.stream) != cudaSuccess ||
+                     cudaMemcpyAsync(sl.h_d, sl.d_d, 4 * (size_t)nq * S->max_k, cudaMemcpyDeviceToHost, sl.stream) !=
+                         cudaSuccess ||
+                     cudaEventRecord(sl.ev, sl.stream) != cudaSuccess))
+                    rc = PK_ERR_CUDA;
+                lk.lock();
+                if (rc != PK_OK) {
+                    for (auto &r : sl.reqs) {
+                        r->status = rc;
+                        r->done = true;
+                        r->t_done = Clock::now();
+                    }
+                    sl.reqs.clear();
+                    sl.offs.clear();
+                    srv_fail_all(S, rc);
+                    continue;
+                }
+                sl.busy = true;
+                sl.t_launch = Clock::now();
+                S->batches++;
+                S->queries += nq;
+                inflight++;
+                S->max_inflight = std::max<int64_t>(S->max_inflight, inflight);
+                did = true;
+            }
+            bool any_busy = false;
+            for (SrvSlot &sl : S->slots) any_busy |= sl.busy;
+            if (!did) {
+                if (any_busy) {
+                    lk.unlock();
+                    std::this_thread::sleep_for(std::chrono::microseconds(20));
+                } else {
+                    S->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+                }
+            }
+        }
+    }
+}
+
+void srv_free(pk_server *S) {
+    for (SrvSlot &sl : S->slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        free_fast_ctx(S->h, sl.ctx);
+        cudaFreeHost(sl.h_q);
+        cudaFreeHost(sl.h_k);
+        cudaFreeHost(sl.h_ef);
+        cudaFreeHost(sl.h_ids);
+        cudaFreeHost(sl.h_d);
+        cudaFree(sl.d_q);
+        cudaFree(sl.d_k);
+        cudaFree(sl.d_ef);
+        cudaFree(sl.d_ids);
+        cudaFree(sl.d_d);
+        if (sl.ev) cudaEventDestroy(sl.ev);
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    delete S;
+}
+
+int srv_create(pk_server **out, pk_index *h, int traversal, int nslots, int32_t max_batch, int32_t max_k,
+               int32_t max_ef, int32_t expand) {
+    if (!out || !h || nslots < 1 || nslots > 64 || max_batch < 1 || max_k < 1 || max_ef < max_k)
+        return fail(PK_ERR_ARG, "bad server arguments (need 1 <= slots <= 64, max_batch >= 1, max_ef >= max_k >= 1)");
+    if (h->n0() == 0) return fail(PK_ERR_STATE, "the index is empty");
+    if (h->trav != (traversal == PK_TRAVERSAL_F16 ? pk::kTravF16 : pk::kTravE4M3)) {
+        int rc = pk_index_prepare_fast_impl(h, traversal);
+        if (rc != PK_OK) return rc;
+    }
+    auto *S = new (std::nothrow) pk_server();
+    if (!S) return fail(PK_ERR_OOM, "host allocation failed");
+    S->h = h;
+    S->max_batch = max_batch;
+    S->max_k = max_k;
+    S->max_ef = max_ef;
+    S->expand = std::max(1, expand);
+    S->slots.resize(nslots);
+    const size_t w = (size_t)(h->dim * h->esz);
+    for (SrvSlot &sl : S->slots) {
+        if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_q, (size_t)max_batch * w) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_k, 4 * (size_t)max_batch) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_ef, 4 * (size_t)max_batch) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_ids, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_d, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_q, (size_t)max_batch * w) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_k, 4 * (size_t)max_batch) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_ef, 4 * (size_t)max_batch) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_ids, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
+            cudaMalloc((void **)&sl.d_d, 4 * (size_t)max_batch * max_k) != cudaSuccess) {
+            cudaGetLastError();
+            srv_free(S);
+            return fail(PK_ERR_OOM, "server buffers could not be allocated");
+        }
+        // grow this slot's scratch to the full batch now, so that serving
+        // allocates nothing: one search of max_batch zero queries
+        std::memset(sl.h_q, 0, (size_t)max_batch * w);
+        for (int32_t i = 0; i < max_batch; i++) {
+            sl.h_k[i] = max_k;
+            sl.h_ef[i] = max_ef;
+        }
+        int rc = PK_OK;
+        if (cudaMemcpy(sl.d_q, sl.h_q, (size_t)max_batch * w, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(sl.d_k, sl.h_k, 4 * (size_t)max_batch, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(sl.d_ef, sl.h_ef, 4 * (size_t)max_batch, cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = fail(PK_ERR_CUDA, "server warm-up copy failed");
+        if (rc == PK_OK)
+            rc = run_search_fast(h, sl.ctx, sl.d_q, false, max_batch, max_k, max_ef, sl.d_k, sl.d_ef, max_k, sl.d_ids,
+                                 sl.d_d, nullptr, S->expand, sl.stream);
+        if (rc == PK_OK && cudaStreamSynchronize(sl.stream) != cudaSuccess) rc = fail(PK_ERR_CUDA, "warm-up failed");
+        if (rc != PK_OK) {
+            srv_free(S);
+            return rc;
+        }
+    }
+    S->worker = std::thread(srv_loop, S);
+    *out = S;
+    return PK_OK;
+}
+
+int srv_submit(pk_server *S, const void *queries, int32_t nq, int32_t k, int32_t ef, int64_t *ticket) {
+    if (!S || !queries || nq < 1 || !ticket) return fail(PK_ERR_ARG, "bad arguments");
+    if (nq > S->max_batch) return fail(PK_ERR_ARG, "request larger than the server's batch capacity");
+    if (k < 1 || k > S->max_k || ef < k || ef > S->max_ef) return fail(PK_ERR_ARG, "k or ef outside the server's limits");
+    auto r = std::make_shared<SrvRequest>();
+    r->nq = nq;
+    r->k = k;
+    r->ef = ef;
+    const size_t bytes = (size_t)nq * (size_t)(S->h->dim * S->h->esz);
+    r->q.assign(static_cast<const uint8_t *>(queries), static_cast<const uint8_t *>(queries) + bytes);
+    r->t_submit = Clock::now();
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->error) return fail(S->error, "the server has failed");
+    r->ticket = S->next_ticket++;
+    *ticket = r->ticket;
+    S->table[r->ticket] = r;
+    S->queue.push_back(std::move(r));
+    S->cv_work.notify_one();
+    return PK_OK;
+}
+
+int srv_wait(pk_server *S, int64_t ticket, int32_t *out_ids, float *out_dists, double *latency_ms,
+             int32_t timeout_ms) {
+    if (!S) return fail(PK_ERR_ARG, "NULL server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->table.find(ticket);
+    if (it == S->table.end()) return fail(PK_ERR_ARG, "unknown ticket");
+    std::shared_ptr<SrvRequest> r = it->second;
+    const auto pred = [&] { return r->done; };
+    if (timeout_ms < 0) {
+        S->cv_done.wait(lk, pred);
+    } else if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) {
+        return fail(PK_ERR_TIMEOUT, "request not finished within the timeout");
+    }
+    S->table.erase(ticket);
+    if (r->status != PK_OK) return fail(r->status, "request failed");
+    if (out_ids) std::memcpy(out_ids, r->ids.data(), 4 * r->ids.size());
+    if (out_dists) std::memcpy(out_dists, r->dists.data(), 4 * r->dists.size());
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    return PK_OK;
+}
+
+}  // namespace
+
 namespace pk {
 // Read-only view of a handle for entry points defined in other files.
 IndexView index_view(const pk_index *h) {
@@ -1224,6 +1770,150 @@ int pk_index_layer(const pk_index *hc, int level, int64_t *n, int64_t *layer_cap
     } catch (...) {
         return fail(PK_ERR_STATE, "pk_index_layer: unknown exception");
     }
+}
+
+int pk_index_prepare_fast(pk_index *h, int traversal) {
+    try {
+        return pk_index_prepare_fast_impl(h, traversal);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_prepare_fast: unexpected exception");
+    }
+}
+
+int pk_index_search_fast(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                         const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride, int32_t *out_ids,
+                         float *out_dists, int32_t *counters, int32_t expand, void *stream) {
+    try {
+        return pk_index_search_fast_impl(h, queries, nq, k, ef, k_per_query, ef_per_query, out_stride, out_ids,
+                                         out_dists, counters, expand, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_search_fast: unexpected exception");
+    }
+}
+
+int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
+                              float *out_dists, int32_t expand) {
+    try {
+        return pk_index_search_fast_host_impl(h, queries, nq, k, ef, out_ids, out_dists, expand);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_search_fast_host: unexpected exception");
+    }
+}
+
+int pk_server_create(pk_server **out, pk_index *h, int traversal, int slots, int32_t max_batch, int32_t max_k,
+                     int32_t max_ef, int32_t expand) {
+    try {
+        return srv_create(out, h, traversal, slots, max_batch, max_k, max_ef, expand);
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_server_create: unexpected exception");
+    }
+}
+
+int pk_server_submit(pk_server *s, const void *queries, int32_t nq, int32_t k, int32_t ef, int64_t *ticket) {
+    try {
+        return srv_submit(s, queries, nq, k, ef, ticket);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_server_submit: unexpected exception");
+    }
+}
+
+int pk_server_wait(pk_server *s, int64_t ticket, int32_t *out_ids, float *out_dists, double *latency_ms,
+                   int32_t timeout_ms) {
+    try {
+        return srv_wait(s, ticket, out_ids, out_dists, latency_ms, timeout_ms);
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_server_wait: unexpected exception");
+    }
+}
+
+int pk_server_stats(pk_server *s, int64_t *out) {
+    if (!s || !out) return fail(PK_ERR_ARG, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out[0] = s->batches;
+    out[1] = s->queries;
+    out[2] = s->max_inflight;
+    out[3] = (int64_t)s->queue.size();
+    out[4] = s->error;
+    return PK_OK;
+}
+
+int pk_server_replay(pk_server *s, const void *queries, int64_t n, const int32_t *nq, const double *arrival_us,
+                     const int32_t *k, const int32_t *ef, int32_t *out_ids, float *out_dists, int32_t out_stride,
+                     double *latency_ms) {
+    if (!s || !queries || n < 0 || !nq || !arrival_us || !k || !ef || !latency_ms || out_stride < 1)
+        return fail(PK_ERR_ARG, "bad arguments");
+    try {
+        const size_t w = (size_t)(s->h->dim * s->h->esz);
+        std::vector<int64_t> tickets(n, 0), qoff(n + 1, 0);
+        for (int64_t i = 0; i < n; i++) qoff[i + 1] = qoff[i] + nq[i];
+        std::atomic<int64_t> submitted{0};
+        std::atomic<int> rc_prod{PK_OK};
+        const auto t0 = Clock::now();
+        std::thread prod([&] {
+            for (int64_t i = 0; i < n; i++) {
+                const auto due = t0 + std::chrono::nanoseconds((int64_t)(arrival_us[i] * 1000.0));
+                while (Clock::now() < due) {
+                }
+                const int rc = srv_submit(s, static_cast<const uint8_t *>(queries) + (size_t)qoff[i] * w, nq[i], k[i],
+                                          ef[i], &tickets[i]);
+                if (rc != PK_OK) {
+                    rc_prod = rc;
+                    break;
+                }
+                submitted.store(i + 1, std::memory_order_release);
+            }
+        });
+        std::vector<int32_t> ids;
+        std::vector<float> ds;
+        int rc = PK_OK;
+        for (int64_t i = 0; i < n && rc == PK_OK; i++) {
+            while (submitted.load(std::memory_order_acquire) <= i && rc_prod == PK_OK) std::this_thread::yield();
+            if (rc_prod != PK_OK) {
+                rc = rc_prod;
+                break;
+            }
+            ids.resize((size_t)nq[i] * k[i]);
+            ds.resize((size_t)nq[i] * k[i]);
+            rc = srv_wait(s, tickets[i], ids.data(), ds.data(), &latency_ms[i], -1);
+            if (rc == PK_OK && out_ids && out_dists)
+                for (int32_t j = 0; j < nq[i]; j++) {
+                    std::memcpy(out_ids + (qoff[i] + j) * out_stride, ids.data() + (size_t)j * k[i], 4 * (size_t)k[i]);
+                    std::memcpy(out_dists + (qoff[i] + j) * out_stride, ds.data() + (size_t)j * k[i],
+                                4 * (size_t)k[i]);
+                }
+        }
+        prod.join();
+        return rc;
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_server_replay: unexpected exception");
+    }
+}
+
+int pk_server_set_watchdog(pk_server *s, double seconds) {
+    if (!s || !(seconds >= 0.0)) return fail(PK_ERR_ARG, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->watchdog_s = seconds;
+    return PK_OK;
+}
+
+int pk_server_destroy(pk_server *s) {
+    if (!s) return PK_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    srv_free(s);
+    return PK_OK;
 }
 
 }  // extern "C"

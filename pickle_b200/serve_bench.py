@@ -1,0 +1,98 @@
+"""Serving benchmark: a Poisson stream of requests through pk_server.
+
+    python -m pickle_b200.serve_bench [--config c2|c5] [--n N] [--rates 20000,50000,...] [--duration 2]
+
+Each request is one query with k uniform in {10, 50, 100} and ef uniform in
+[max(k, 32), 256]; arrivals are a Poisson process at each rate (requests per
+second).  The stream is replayed by the library's native replayer
+(pk_server_replay) against a continuous-batching server (slots overlapping on
+the GPU, batches of up to --max-batch queries).  Reported per rate: offered
+and served requests/s, p50/p99/max latency (submit to results on the host)
+and recall@10 of the served results against exact float64 ground truth.
+Data are seeded synthetic stand-ins for the configuration's shapes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+
+def gt_torch(base, queries, k, metric, device):
+    import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
+    b = torch.from_numpy(base).to(device).float()
+    out = np.empty((len(queries), k), np.int64)
+    bn = (b * b).sum(1) if metric == "l2" else None
+    for i in range(0, len(queries), 512):
+        q = torch.from_numpy(queries[i:i + 512]).to(device).float()
+        s = -(q @ b.T) if metric == "ip" else (q * q).sum(1)[:, None] + bn[None, :] - 2 * q @ b.T
+        top = torch.topk(s, k + 32, dim=1, largest=False).indices
+        qd, bd = q.double(), b[top].double()
+        s64 = -(qd[:, None, :] * bd).sum(-1) if metric == "ip" else ((qd[:, None, :] - bd) ** 2).sum(-1)
+        order = torch.argsort(s64, dim=1, stable=True)[:, :k]
+        out[i:i + 512] = torch.gather(top, 1, order).cpu().numpy()
+    return out
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--config", default="c2", choices=["c2", "c5"])
+    p.add_argument("--n", type=int, default=0)
+    p.add_argument("--pool", type=int, default=20000, help="distinct queries the stream samples from")
+    p.add_argument("--rates", default="20000,50000,100000,200000")
+    p.add_argument("--duration", type=float, default=2.0, help="seconds of arrivals per rate")
+    p.add_argument("--slots", type=int, default=4)
+    p.add_argument("--max-batch", type=int, default=4096)
+    p.add_argument("--traversal", default="f16", choices=["f16", "fp8"])
+    p.add_argument("--M", type=int, default=0)
+    p.add_argument("--efc", type=int, default=0)
+    p.add_argument("--seed", type=int, default=0)
+    a = p.parse_args(argv)
+
+    import torch
+
+    from pickle_b200 import HNSWIndex, Server, datasets
+    if a.config == "c2":
+        n, dim, metric, M, efc = a.n or 1_000_000, 96, "ip", a.M or 32, a.efc or 400
+        base, _ = datasets.gmm_unit(n, 0, dim, ncomp=256, sigma=0.3, seed=a.seed)
+        _, pool = datasets.gmm_unit(0, a.pool, dim, ncomp=256, sigma=0.3, seed=a.seed)
+    else:
+        n, dim, metric, M, efc = a.n or 5_000_000, 768, "ip", a.M or 48, a.efc or 200
+        base, _ = datasets.gmm_unit(n, 0, dim, ncomp=2048, sigma=0.3, seed=a.seed, dtype=np.float16, zipf_s=1.1)
+        _, pool = datasets.gmm_unit(0, a.pool, dim, ncomp=2048, sigma=0.3, seed=a.seed, dtype=np.float16, zipf_s=1.1)
+    idx = HNSWIndex(dim, base.dtype, metric, M=M, ef_construction=efc)
+    idx.set_seed(a.seed)
+    t0 = time.time()
+    idx.build(base)
+    build_s = time.time() - t0
+    idx.prepare_fast(a.traversal)
+    gt = gt_torch(base, pool, 10, metric, torch.device("cuda"))
+    srv = Server(idx, a.traversal, slots=a.slots, max_batch=a.max_batch, max_k=100, max_ef=256)
+    rng = np.random.default_rng(a.seed + 1)
+    for rate in [float(x) for x in a.rates.split(",")]:
+        nreq = max(1, int(rate * a.duration))
+        arrival = np.cumsum(rng.exponential(1e6 / rate, size=nreq))
+        sel = rng.integers(0, len(pool), size=nreq)
+        k = rng.choice([10, 50, 100], size=nreq).astype(np.int32)
+        ef = np.array([rng.integers(max(kk, 32), 257) for kk in k], np.int32)
+        ids, _, lat = srv.replay(pool[sel], np.ones(nreq, np.int32), arrival, k, ef, out_stride=100)
+        done = arrival / 1e3 + lat
+        span_ms = done.max() - arrival[0] / 1e3
+        rec = datasets.recall_at_k(ids[:, :10], gt[sel], 10)
+        st = srv.stats()
+        print(json.dumps({
+            "config": a.config, "n": n, "dim": dim, "metric": metric, "M": M, "ef_construction": efc,
+            "traversal": a.traversal, "slots": a.slots, "max_batch": a.max_batch, "build_s": round(build_s, 1),
+            "offered_req_per_s": rate, "requests": nreq, "served_req_per_s": round(nreq / (span_ms / 1e3), 1),
+            "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                           "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3)},
+            "recall_at_10": round(rec, 4), "k": "uniform {10,50,100}", "ef": "uniform [max(k,32), 256]",
+            "server": st}), flush=True)
+    srv.close()
+
+
+if __name__ == "__main__":
+    main()
