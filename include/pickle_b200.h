@@ -130,7 +130,7 @@ int pk_index_prepare_fast(pk_index *h, int traversal);
  * vectors (the returned distances are exact; the ids may differ from the
  * exact search's where low-precision distances reorder the walk).  Arguments
  * as pk_index_search_device; `ef` bounds ef_per_query; expand = list entries
- * expanded per step (1..4, 0 = 1).  Fully asynchronous on `stream` (no host
+ * expanded per step (1..4, 0 = 1); ef <= 512.  Fully asynchronous on `stream` (no host
  * synchronisation), so it can be captured in a CUDA graph once buffers have
  * grown to the batch size by an earlier call.  Successive calls on one
  * handle share its scratch: order them on one stream. */
@@ -139,9 +139,18 @@ int pk_index_search_fast(pk_index *h, const void *queries, int64_t nq, int32_t k
                          int32_t *out_ids, float *out_dists, int32_t *counters, int32_t expand, void *stream);
 
 /* pk_index_search_fast with host buffers (queries nq*dim in, out_ids /
- * out_dists nq*k out); synchronous. */
+ * out_dists nq*k out); synchronous.  PK_ERR_TIMEOUT if a row fetch of the
+ * walk did not complete within its bound (the results are then -1). */
 int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
                               float *out_dists, int32_t expand);
+
+/* Launch shape of pk_index_search_fast's walk (0 keeps the default):
+ * rows_per_batch = vector rows fetched per round trip (1..256; default
+ * min(32, 12 KiB / row)); filter_log2 = log2 of the slots of the per-query
+ * table of recently seen ids (5..15; default 10); warps_per_block (1..8;
+ * default 4).  The results do not depend on the shape (the table only saves
+ * recomputed distances); the speed does.  No counterpart in the reference. */
+int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter_log2, int32_t warps_per_block);
 
 /* Serving: continuous batching over pk_index_search_fast.  No counterpart
  * in the reference (its batch AnnSearch is a blocking OpenMP loop,

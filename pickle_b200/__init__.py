@@ -69,6 +69,7 @@ def lib() -> ctypes.CDLL:
         L.pk_index_prepare_fast.argtypes = [P, ctypes.c_int]
         L.pk_index_search_fast.argtypes = [P, VP, I64, I32, I32, VP, VP, I32, VP, VP, VP, I32, VP]
         L.pk_index_search_fast_host.argtypes = [P, VP, I64, I32, I32, VP, VP, I32]
+        L.pk_index_set_fast_params.argtypes = [P, I32, I32, I32]
         L.pk_index_search_noalloc.argtypes = [P, VP, I64, I32, I32, VP, VP, VP]
         L.pk_server_create.argtypes = [PP, P, ctypes.c_int, ctypes.c_int, I32, I32, I32, I32]
         L.pk_server_submit.argtypes = [P, VP, I32, I32, I32, ctypes.POINTER(ctypes.c_int64)]
@@ -186,6 +187,11 @@ class HNSWIndex:
     def prepare_fast(self, traversal: str = "fp8") -> None:
         """Build the FP16 / FP8 (per-dimension scaled) copy the fast search walks with."""
         _check(lib().pk_index_prepare_fast(self._h, self.TRAVERSAL[traversal]))
+
+    def set_fast_params(self, rows_per_batch: int = 0, filter_log2: int = 0, warps_per_block: int = 0) -> None:
+        """Launch shape of the fast walk (0 = default): rows fetched per round trip, log2 of the
+        recently-seen-id table's slots, warps per block.  Results do not depend on the shape."""
+        _check(lib().pk_index_set_fast_params(self._h, rows_per_batch, filter_log2, warps_per_block))
 
     def search_fast_device(self, queries, k: int, ef: int, out_ids, out_dists, k_per_query=None, ef_per_query=None,
                            counters=None, expand: int = 1, stream=None) -> None:

@@ -2,26 +2,38 @@
 //
 // The exact kernel (pk_search.cu) replays the reference's binary heaps with
 // one lane, which is what makes its ids bit-identical to the reference's but
-// also what bounds it.  This kernel answers the same question - the k nearest
-// neighbours found by a best-first walk of the HNSW graph with a result set
-// of ef entries (include/hnsw.hpp:373-444) - with data structures suited to a
-// warp, and is judged by recall:
+// also what bounds it.  These kernels answer the same question - the k
+// nearest neighbours found by a best-first walk of the HNSW graph with a
+// result set of ef entries (include/hnsw.hpp:373-444) - with data structures
+// suited to a warp, and are judged by recall.  Two launches per batch:
+//
+// walk_kernel (one query per warp, work stealing, per-query ef):
 //   * traversal distances come from a low-precision copy of the vectors:
-//     FP16, or FP8 E4M3 scaled per dimension (a query is scaled by the same
-//     per-dimension factors; for L2 a per-row norm of the scaled copy turns
-//     the distance into a dot product), always accumulated in FP32;
-//   * the result set is a sorted list of ef slots in shared memory (distance,
-//     id, expanded flag) instead of two heaps; each iteration expands the P
-//     best unexpanded entries at once, marks their neighbours in the exact
-//     visited bitmap, stages the new rows with cp.async, sorts the new
-//     candidates with a warp bitonic sort and merges them into the list;
-//   * the walk ends when every listed entry is expanded; the listed entries
-//     (the top ef) are then re-ranked with exact distances from the original
-//     vectors and the k best are written, closest first (ties by id).
-// Upper layers are descended greedily as in SlideLayer (include/hnsw.hpp:446-494),
-// with traversal distances.  Queries run one per warp with work stealing and
-// may have different k and ef.  There is no host round trip, so a batch can
-// be captured in a CUDA graph.
+//     FP16 (dot products on the tensor cores), or FP8 E4M3 scaled per
+//     dimension (a query is scaled by the same per-dimension factors); for L2
+//     the stored per-row norms turn the distance into a dot product;
+//   * upper layers are descended greedily as in SlideLayer
+//     (include/hnsw.hpp:446-494);
+//   * on layer 0 the result set is a sorted list of ef entries held in
+//     registers (lane l owns entries l*S .. l*S+S-1); each iteration expands
+//     the `expand` best unexpanded entries, filters their neighbours through
+//     a small direct-mapped table of recently seen ids in shared memory,
+//     fetches the new rows with one bulk copy (cp.async.bulk) per row onto a
+//     per-warp mbarrier, and inserts what beats the worst listed entry;
+//   * the walk ends when the first ef entries are all expanded, and their
+//     ids are written out.
+//   The visited table forgets ids on collisions, which costs a recomputed
+//   distance but never a duplicate: an insertion of an id the list holds is
+//   dropped, and a node that left the list (or was turned away) cannot come
+//   back, since the worst listed distance never rises.  So the list after
+//   each step - the best ef of what was listed and what was met - does not
+//   depend on the table's size or on the batch order.
+//
+// rerank_kernel (one query per warp): exact distances from the original
+// vectors for the ef listed ids, sorted by (distance, id); the k best are
+// written with their external ids.
+//
+// There is no host round trip, so a batch can be captured in a CUDA graph.
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
 
@@ -37,32 +49,28 @@ using namespace dev;
 constexpr uint32_t kExpanded = 0x80000000u;
 
 // ------------------------------------------------------- traversal distances
-// Lane layout for traversal rows: CT 16-byte chunks per row, GT lanes per row
-// (power of two >= CT, at most 32), KT chunks per lane.
+// E4M3 lane layout: CT 16-byte chunks per row, GT lanes per row (power of
+// two >= CT, at most 32), KT chunks per lane.
 
 struct TravCfg {
     int GT, KT, CT;
 };
 
-// F16 traversal: the query is held as halves, accumulated in FP32 (Acc<F16>).
+// FP16 traversal: rows and queries are stored divided by one power of two
+// that brings the largest stored magnitude into [4, 8) (a power of two
+// changes no rounding and no order of distances).  Dot products run on the
+// tensor cores (trav_dist_buf); the query is staged in shared memory.
 // E4M3 traversal: the query is held as 16 floats per chunk (pre-scaled).
 template <int TRAV, int KT>
 struct TravQuery;
 
 template <int KT>
-struct TravQuery<kTravF16, KT> {
-    uint4 q[KT];
-    __device__ __forceinline__ float dot_or_l2(const uint4 &r, int k, bool ip) const {
-        float a = 0.f;
-        Acc<PK_DTYPE_F16>::add(a, q[k], r, ip);
-        return a;
-    }
-};
+struct TravQuery<kTravF16, KT> {};
 
 template <int KT>
 struct TravQuery<kTravE4M3, KT> {
     float q[KT][16];
-    __device__ __forceinline__ float dot_or_l2(const uint4 &r, int k, bool) const {
+    __device__ __forceinline__ float dot(const uint4 &r, int k) const {
         const uint32_t w[4] = {r.x, r.y, r.z, r.w};
         float a = 0.f;
 #pragma unroll
@@ -85,130 +93,537 @@ struct TravView {
     const uint8_t *rows;      // traversal copy, row_bytes apart
     const uint8_t *zero_row;
     int64_t row_bytes;
-    const float *rownorm;     // E4M3 + L2: sum_d (s_d x_d)^2 of the stored row
+    const float *rownorm;     // L2: sum of squares of the stored row's values
     __device__ __forceinline__ const uint8_t *row(int32_t r) const {
         return r >= 0 ? rows + (int64_t)r * row_bytes : zero_row;
     }
 };
 
-// Traversal distance of nrows rows (<= 32) staged kStageRows at a time.
+// ------------------------------------------------------ asynchronous rows --
+// Rows move from global to shared memory with one bulk copy per row, issued
+// by as many lanes as there are rows and completing on a per-warp mbarrier
+// that counts the bytes.  A warp waits once per batch of rows.
+
+constexpr int kWaitPolls = 1 << 20;  // bound on mbarrier polls for one batch
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_poll(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+struct RowFetch {
+    uint8_t *buf;    // row t lands at buf + t * stride
+    int64_t stride;
+    uint64_t *bar;
+    uint32_t parity;
+};
+
+// Copies rows[0..n) of the traversal copy (n >= 1; each a row index below the
+// copy's row count, or -1 for the zero row) into f.buf.  With norm_out, the
+// rows' stored norms go to norm_out[t].  All lanes call.  Returns false on
+// every lane if the copies did not land within the poll bound; the copies are
+// then given one more bounded wait before returning.
+__device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, const int32_t *rows, int n,
+                                           float *norm_out, int lane) {
+    __syncwarp();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lane == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(f.bar)),
+                     "r"((uint32_t)(n * tv.row_bytes))
+                     : "memory");
+    __syncwarp();
+    for (int t = lane; t < n; t += 32) {
+        const int32_t r = rows[t];
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(f.buf + t * f.stride)),
+            "l"(tv.row(r)), "r"((uint32_t)tv.row_bytes), "r"(smem_u32(f.bar))
+            : "memory");
+        if (norm_out) norm_out[t] = r >= 0 ? tv.rownorm[r] : 0.f;
+    }
+    bool ok = false;
+    for (int i = 0; i < kWaitPolls && !ok; i++) ok = mbar_poll(f.bar, f.parity);
+    const bool all = __all_sync(kFull, ok);
+    if (!all && !ok)
+        for (int i = 0; i < kWaitPolls && !ok; i++) ok = mbar_poll(f.bar, f.parity);
+    f.parity ^= 1u;
+    __syncwarp();
+    return all;
+}
+
+// Traversal distances of the n staged rows to the query, into cd[t] (for L2,
+// cd[t] holds the row's stored norm on entry).  All lanes call.
+//
+// FP16: the tensor cores.  Sixteen staged rows at a time are the A operand of
+// mma.m16n8k16 (ldmatrix takes one row address per lane, so the gathered rows
+// need no particular layout), the query is column 0 of B (lanes 0-3 hold its
+// fragment; B's other columns are zero), and column 0 of the FP32
+// accumulator holds the 16 dot products.  L2 = |q|^2 + |x|^2 - 2 q.x from
+// the stored norms of the same FP16 values.
+// E4M3: groups of G lanes per row, FP32 FMAs over the decoded elements.
 template <int TRAV, int KT>
-__device__ __forceinline__ void trav_dist_rows(const TravView &tv, const TravCfg &tc, const TravQuery<TRAV, KT> &tq,
-                                               bool ip, float qnorm, const int32_t *rows, float *outd, int nrows,
-                                               uint8_t *rowbuf, int lane) {
-    const int G = tc.GT, R = 32 / G, grp = lane / G, gl = lane % G;
-    for (int b0 = 0; b0 < nrows; b0 += kStageRows) {
-        const int nb = min(kStageRows, nrows - b0);
-        for (int t = grp; t < nb; t += R) {
-            const uint8_t *src = tv.row(rows[b0 + t]);
-            uint8_t *dst = rowbuf + (int64_t)t * tv.row_bytes;
-#pragma unroll
-            for (int k = 0; k < KT; k++) {
-                const int c = gl + k * G;
-                if (c < tc.CT) cp_async16(dst + c * 16, src + c * 16);
+__device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery<TRAV, KT> &tq, bool ip, float qnorm,
+                                              const RowFetch &f, int64_t row_bytes, const uint8_t *qbuf, float *cd,
+                                              int n, int lane) {
+    if constexpr (TRAV == kTravF16) {
+        const int ks = (int)(row_bytes / 32);
+        const uint32_t *qw = reinterpret_cast<const uint32_t *>(qbuf);
+        for (int t0 = 0; t0 < n; t0 += 16) {
+            const int r = min(t0 + (lane & 15), n - 1);
+            const uint32_t arow = smem_u32(f.buf + r * f.stride) + (uint32_t)(lane >> 4) * 16u;
+            float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+            for (int kk = 0; kk < ks; kk++) {
+                uint32_t a0, a1, a2, a3;
+                asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                             : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+                             : "r"(arow + (uint32_t)kk * 32u)
+                             : "memory");
+                uint32_t b0 = 0, b1 = 0;
+                if (lane < 4) {
+                    b0 = qw[kk * 8 + lane];
+                    b1 = qw[kk * 8 + 4 + lane];
+                }
+                asm volatile(
+                    "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                    "{%0, %1, %2, %3};"
+                    : "+f"(c0), "+f"(c1), "+f"(c2), "+f"(c3)
+                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+            }
+            // column 0: lanes 4g hold rows t0 + g (c0) and t0 + g + 8 (c2)
+            if ((lane & 3) == 0) {
+                const int ra = t0 + (lane >> 2), rb = ra + 8;
+                if (ra < n) cd[ra] = ip ? -c0 : qnorm + cd[ra] - 2.f * c0;
+                if (rb < n) cd[rb] = ip ? -c2 : qnorm + cd[rb] - 2.f * c2;
             }
         }
-        cp_async_wait_all();
-        for (int base = 0; base < nb; base += R) {
+    } else {
+        const int G = tc.GT, R = 32 / G, grp = lane / G, gl = lane % G;
+        for (int base = 0; base < n; base += R) {
             const int t = base + grp;
             float acc = 0.f;
-            if (t < nb) {
-                const uint8_t *row = rowbuf + (int64_t)t * tv.row_bytes;
+            if (t < n) {
+                const uint8_t *row = f.buf + t * f.stride;
 #pragma unroll
                 for (int k = 0; k < KT; k++) {
                     const int c = gl + k * G;
-                    if (c < tc.CT) acc += tq.dot_or_l2(*reinterpret_cast<const uint4 *>(row + c * 16), k, ip);
+                    if (c < tc.CT) acc += tq.dot(*reinterpret_cast<const uint4 *>(row + c * 16), k);
                 }
             }
             for (int off = G >> 1; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off);
-            if (gl == 0 && t < nb) {
-                float d;
-                if constexpr (TRAV == kTravF16) {
-                    d = ip ? -acc : acc;
-                } else {
-                    const int32_t r = rows[b0 + t];
-                    d = ip ? -acc : qnorm - 2.f * acc + (r >= 0 ? tv.rownorm[r] : 0.f);
+            if (gl == 0 && t < n) cd[t] = ip ? -acc : qnorm - 2.f * acc + cd[t];
+        }
+    }
+    __syncwarp();
+}
+
+// Appends this warp's new entries (lanes with ok, in lane order) to the
+// pending batch crow/cid at n, flushing the batch whenever rb entries wait.
+// Returns false if a flush failed.
+template <class Flush>
+__device__ __forceinline__ bool append_pending(bool ok, int32_t id, int32_t row, int32_t *crow, int32_t *cid, int &n,
+                                               int rb, int lane, Flush &flush) {
+    const unsigned m = __ballot_sync(kFull, ok);
+    const int total = __popc(m);
+    const int rank = __popc(m & ((1u << lane) - 1u));
+    int done = 0;
+    while (done < total) {
+        if (n == rb) {
+            __syncwarp();
+            if (!flush(n)) return false;
+            n = 0;
+        }
+        const int take = min(rb - n, total - done);
+        if (ok && rank >= done && rank < done + take) {
+            crow[n + rank - done] = row;
+            cid[n + rank - done] = id;
+        }
+        n += take;
+        done += take;
+    }
+    __syncwarp();
+    return true;
+}
+
+// ------------------------------------------------------------ result list --
+// The ef best entries found so far, sorted by (distance, id), in registers:
+// lane l holds entries l*S .. l*S+S-1.  Empty slots hold (+inf, kEmpty); the
+// top bit of an id marks an entry already expanded.
+
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+__device__ __forceinline__ bool key_less(float da, uint32_t ia, float db, uint32_t ib) {
+    return da < db || (da == db && ia < ib);
+}
+
+template <int S>
+struct RegList {
+    float d[S];
+    uint32_t id[S];
+
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            d[s] = __int_as_float(0x7f800000);
+            id[s] = kEmpty;
+        }
+    }
+
+    // Inserts (nd, nid) (nid without the flag; nd finite) at its rank unless
+    // the list holds nid already; the last entry of the 32*S falls off.
+    __device__ __forceinline__ void insert(float nd, uint32_t nid, int lane) {
+        int c = 0;
+        bool dup = false;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            const uint32_t m = id[s] & ~kExpanded;
+            c += key_less(d[s], m, nd, nid) ? 1 : 0;
+            dup |= m == nid;
+        }
+        if (__any_sync(kFull, dup)) return;
+        // sorted: lanes before the rank have c == S, lanes after it c == 0
+        const float pd = __shfl_up_sync(kFull, d[S - 1], 1);
+        const uint32_t pi = __shfl_up_sync(kFull, id[S - 1], 1);
+        const int pc = __shfl_up_sync(kFull, c, 1);
+        const bool here = c > 0 || lane == 0 || pc == S;  // the new entry lands in slot c of this lane
+        if (c < S) {
+#pragma unroll
+            for (int s = S - 1; s >= 0; s--) {
+                if (s > 0 && s > c) {
+                    d[s] = d[s - 1];
+                    id[s] = id[s - 1];
+                } else if (s == c) {
+                    d[s] = here ? nd : pd;
+                    id[s] = here ? nid : pi;
                 }
-                outd[b0 + t] = d;
             }
         }
     }
-}
 
-// ------------------------------------------------------------ sorted list --
-// Entries order by (distance, id), the expanded flag masked off.
-__device__ __forceinline__ bool ent_less(float da, uint32_t ia, float db, uint32_t ib) {
-    return da < db || (da == db && (ia & ~kExpanded) < (ib & ~kExpanded));
-}
-
-// Bitonic sort of one (d, id) pair per lane, ascending across the warp.
-__device__ __forceinline__ void warp_sort32(float &d, uint32_t &id, int lane) {
+    // Marks the first unexpanded entry among the slots in vmask as expanded
+    // and returns its id, or -1 if there is none.
+    __device__ __forceinline__ int32_t take_first(unsigned vmask, int lane) {
+        unsigned un = 0;
 #pragma unroll
-    for (int size = 2; size <= 32; size <<= 1) {
+        for (int s = 0; s < S; s++) un |= ((id[s] & kExpanded) == 0 ? 1u : 0u) << s;
+        un &= vmask;
+        const unsigned b = __ballot_sync(kFull, un != 0);
+        if (b == 0) return -1;
+        const int fl = __ffs(b) - 1;
+        int32_t v = 0;
+        if (lane == fl) {
+            const int fs = __ffs(un) - 1;
 #pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            const float od = __shfl_xor_sync(kFull, d, stride);
-            const uint32_t oi = __shfl_xor_sync(kFull, id, stride);
-            const bool up = ((lane & size) == 0);
-            const bool lower = (lane & stride) == 0;
-            // the lower lane keeps the smaller entry in an ascending run
-            const bool take_other = lower == up ? ent_less(od, oi, d, id) : ent_less(d, id, od, oi);
-            if (take_other) {
-                d = od;
-                id = oi;
-            }
+            for (int s = 0; s < S; s++)
+                if (s == fs) {
+                    v = (int32_t)id[s];
+                    id[s] |= kExpanded;
+                }
         }
+        return __shfl_sync(kFull, v, fl);
     }
-}
 
-struct ListBuf {
-    float *d;
-    uint32_t *id;
+    // The entry in slot ws of lane wl (distance, id without the flag).
+    __device__ __forceinline__ void at(int wl, int ws, float &wd, uint32_t &wi, int lane) const {
+        float x = 0.f;
+        uint32_t y = 0;
+        if (lane == wl) {
+#pragma unroll
+            for (int s = 0; s < S; s++)
+                if (s == ws) {
+                    x = d[s];
+                    y = id[s] & ~kExpanded;
+                }
+        }
+        wd = __shfl_sync(kFull, x, wl);
+        wi = __shfl_sync(kFull, y, wl);
+    }
 };
 
-// Merge up to 32 sorted new entries (one per lane: nd/nid, +inf padded) into
-// the sorted list src[0..cnt), writing the first L of the union to dst.
-// Returns the new count.  newd/newid: shared scratch of 32 entries.
-__device__ __forceinline__ int merge_into(const ListBuf &src, const ListBuf &dst, int cnt, int L, float nd,
-                                          uint32_t nid, int m, float *newd, uint32_t *newid, int lane) {
-    newd[lane] = nd;
-    newid[lane] = nid;
-    __syncwarp();
-    // list entries: new position = i + #new entries before them
-    for (int i = lane; i < cnt; i += 32) {
-        const float d = src.d[i];
-        const uint32_t id = src.id[i];
-        int lo = 0, hi = m;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (ent_less(newd[mid], newid[mid], d, id)) lo = mid + 1;
-            else hi = mid;
-        }
-        const int p = i + lo;
-        if (p < L) {
-            dst.d[p] = d;
-            dst.id[p] = id;
+// Argmin over (cd[t], t), t < n: the first of the smallest distances.
+__device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, int &bt, int lane) {
+    float d = __int_as_float(0x7f800000);
+    int t = 0x7fffffff;
+    for (int i = lane; i < n; i += 32) {
+        const float x = cd[i];
+        if (x < d) {
+            d = x;
+            t = i;
         }
     }
-    // new entries: position = lane + #list entries before them
-    if (lane < m) {
-        int lo = 0, hi = cnt;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (ent_less(src.d[mid], src.id[mid], nd, nid)) lo = mid + 1;
-            else hi = mid;
-        }
-        const int p = lane + lo;
-        if (p < L) {
-            dst.d[p] = nd;
-            dst.id[p] = nid;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float od = __shfl_xor_sync(kFull, d, off);
+        const int ot = __shfl_xor_sync(kFull, t, off);
+        if (od < d || (od == d && ot < t)) {
+            d = od;
+            t = ot;
         }
     }
-    __syncwarp();
-    return min(L, cnt + m);
+    bd = d;
+    bt = t;
 }
 
-// Bitonic sort of n (power of two, <= 2*list size) entries in shared memory.
+// ------------------------------------------------------------------ walk ---
+// Narrow lists (ef <= 128) fit 80 registers per thread without spills, so
+// three 256-thread blocks can be resident per SM; wider lists, and E4M3
+// queries of more than one chunk per lane, take two.
+template <int TRAV, int KT, int S>
+__global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1)) ? 3 : 2)
+    walk_kernel(const DevGraph *__restrict__ gp, const TravCfg tc, const WalkArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const WalkLayout lay = walk_layout(a.rb, a.trav_row_bytes, a.hlog2);
+    unsigned char *my = smem + (size_t)wib * lay.total;
+    int32_t *tab = reinterpret_cast<int32_t *>(my + lay.tab);
+    int32_t *crow = reinterpret_cast<int32_t *>(my + lay.crow);
+    int32_t *cid = reinterpret_cast<int32_t *>(my + lay.cid);
+    float *cd = reinterpret_cast<float *>(my + lay.cd);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(my + lay.bar);
+    if (lane == 0) mbar_init(bar);
+    __syncwarp();
+    uint8_t *qbuf = my + lay.qbuf;
+    RowFetch f{my + lay.rowbuf, lay.stride, bar, 0u};
+
+    const TravView tv{a.trav, a.trav_zero, a.trav_row_bytes, a.rownorm};
+    const bool ip = gp->metric == PK_METRIC_IP;
+    float *const norm_out = ip ? nullptr : cd;
+    const int enter_level = gp->enter_level;
+    const int rb = a.rb;
+    const int H = 1 << a.hlog2;
+    const int hshift = 32 - a.hlog2;
+    const int expand = max(1, min(a.expand, 4));
+    const DevLayer L0 = gp->L[0];
+    const int64_t lim0 = min(L0.lcap, a.trav_rows);
+    const float kInf = __int_as_float(0x7f800000);
+
+    for (;;) {
+        int qi = 0;
+        if (lane == 0) qi = atomicAdd(a.work, 1);
+        qi = __shfl_sync(kFull, qi, 0);
+        if (qi >= a.nq) break;
+        const int64_t q = qi;
+        const int L = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, 32 * S));
+
+        // the query in the traversal format: FP16 staged in shared memory,
+        // E4M3 as this lane's chunks in registers
+        TravQuery<TRAV, KT> tq;
+        const float qnorm = ip ? 0.f : a.qnorm[q];
+        {
+            const uint8_t *qrow = a.tq_rows + q * a.tq_row_bytes;
+            if constexpr (TRAV == kTravF16) {
+                for (int c = lane; c < (int)(a.tq_row_bytes / 16); c += 32)
+                    reinterpret_cast<uint4 *>(qbuf)[c] = ld16(qrow + c * 16);
+                __syncwarp();
+            } else {
+                const int G = tc.GT, gl = lane % G;
+#pragma unroll
+                for (int kk = 0; kk < KT; kk++) {
+                    const int c = gl + kk * G;
+#pragma unroll
+                    for (int e = 0; e < 16; e++) tq.q[kk][e] = 0.f;
+                    if (c < tc.CT) {
+                        const float *qf = reinterpret_cast<const float *>(qrow) + c * 16;
+#pragma unroll
+                        for (int e = 0; e < 16; e++) tq.q[kk][e] = qf[e];
+                    }
+                }
+            }
+        }
+
+        int32_t cnt[6] = {0, 0, 0, 0, 0, 0};
+        bool failed = false;
+
+        // ---- upper layers: greedy descent with traversal distances ----
+        int32_t enter = gp->L[enter_level].ent;
+        for (int level = enter_level; level >= 1 && !failed; --level) {
+            const DevLayer Ly = gp->L[level];
+            auto vrow = [&](int32_t v) -> int32_t {
+                const int32_t r = Ly.vrow[v];
+                return r < a.trav_rows ? r : -1;
+            };
+            if (lane == 0) crow[0] = vrow(enter);
+            if (!fetch_rows(f, tv, crow, 1, norm_out, lane)) {
+                failed = true;
+                break;
+            }
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, 1, lane);
+            float best = cd[0];
+            int32_t c = enter;
+            bool moved = false;
+            auto flush_up = [&](int nn) -> bool {
+                if (!fetch_rows(f, tv, crow, nn, norm_out, lane)) return false;
+                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, nn, lane);
+                float bd;
+                int bt;
+                warp_argmin(cd, nn, bd, bt, lane);
+                if (bd < best) {
+                    best = bd;
+                    c = cid[bt];
+                    moved = true;
+                }
+                cnt[1] += nn;
+                __syncwarp();
+                return true;
+            };
+            for (int64_t round = 0; round <= Ly.lcap; round++) {
+                const int64_t base = (int64_t)c * Ly.cap;
+                const int deg = Ly.deg[c];
+                cnt[0]++;
+                cnt[2] += deg;
+                moved = false;
+                int n = 0;
+                for (int j0 = 0; j0 < deg && !failed; j0 += 32) {
+                    const int j = j0 + lane;
+                    const int32_t v = j < deg ? Ly.adj[base + j] : -1;
+                    const bool ok = v >= 0 && v < Ly.lcap;
+                    const int32_t r = ok ? vrow(v) : -1;
+                    if (!append_pending(ok, v, r, crow, cid, n, rb, lane, flush_up)) failed = true;
+                }
+                if (!failed && n > 0 && !flush_up(n)) failed = true;
+                if (failed || !moved) break;
+            }
+            const int32_t dn = Ly.down[c];
+            enter = dn >= 0 ? dn : gp->L[level - 1].ent;
+        }
+
+        // ---- layer 0: best-first walk over the register list ----
+        RegList<S> list;
+        list.clear();
+        const int wl = (L - 1) / S, wsl = (L - 1) % S;
+        const int own = L - lane * S;  // slots of this lane below L
+        const unsigned vmask = own <= 0 ? 0u : own >= S ? (S >= 32 ? ~0u : (1u << S) - 1u) : (1u << own) - 1u;
+        float wd = kInf;
+        uint32_t wi = kEmpty & ~kExpanded;
+        if (!failed) {
+            for (int i = lane * 4; i < H; i += 128)
+                *reinterpret_cast<int4 *>(tab + i) = make_int4(-1, -1, -1, -1);
+            if (enter < 0 || enter >= lim0) enter = 0;
+            if (lane == 0) crow[0] = enter;
+            if (!fetch_rows(f, tv, crow, 1, norm_out, lane)) failed = true;
+        }
+        if (!failed) {
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, 1, lane);
+            const float d0 = cd[0];
+            if (lane == 0) {
+                list.d[0] = d0;
+                list.id[0] = (uint32_t)enter;
+                tab[((uint32_t)enter * 2654435769u) >> hshift] = enter;
+            }
+            __syncwarp();
+            list.at(wl, wsl, wd, wi, lane);
+        }
+        auto flush0 = [&](int nn) -> bool {
+            if (!fetch_rows(f, tv, crow, nn, norm_out, lane)) return false;
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, nn, lane);
+            cnt[4] += nn;
+            for (int i0 = 0; i0 < nn; i0 += 32) {
+                const int i = i0 + lane;
+                float nd = kInf;
+                uint32_t nid = kEmpty;
+                if (i < nn) {
+                    nd = cd[i];
+                    nid = (uint32_t)crow[i];
+                }
+                unsigned m = __ballot_sync(kFull, i < nn && nd < kInf && key_less(nd, nid, wd, wi));
+                while (m) {
+                    const int src = __ffs(m) - 1;
+                    m &= m - 1;
+                    const float xd = __shfl_sync(kFull, nd, src);
+                    const uint32_t xi = __shfl_sync(kFull, nid, src);
+                    if (!key_less(xd, xi, wd, wi)) continue;
+                    list.insert(xd, xi, lane);
+                    list.at(wl, wsl, wd, wi, lane);
+                }
+            }
+            __syncwarp();
+            return true;
+        };
+        int64_t iters = 0;
+        while (!failed) {
+            int32_t pc[4];
+#pragma unroll
+            for (int p = 0; p < 4; p++) pc[p] = p < expand ? list.take_first(vmask, lane) : -1;
+            if (pc[0] < 0 || ++iters > L0.lcap) break;
+            // degrees and the first 64 slots of each parent's list, all in flight
+            int pdeg[4];
+            int32_t pa0[4], pa1[4];
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                pdeg[p] = 0;
+                pa0[p] = -1;
+                pa1[p] = -1;
+                if (pc[p] >= 0) {
+                    const int64_t base = (int64_t)pc[p] * L0.cap;
+                    pdeg[p] = L0.deg[pc[p]];
+                    if (lane < L0.cap) pa0[p] = L0.adj[base + lane];
+                    if (32 + lane < L0.cap) pa1[p] = L0.adj[base + 32 + lane];
+                }
+            }
+            int n = 0;
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                if (pc[p] < 0 || failed) continue;
+                const int deg = pdeg[p];
+                const int64_t base = (int64_t)pc[p] * L0.cap;
+                cnt[3]++;
+                cnt[5] += deg;
+                for (int j0 = 0; j0 < deg; j0 += 32) {
+                    const int j = j0 + lane;
+                    int32_t v = -1;
+                    if (j < deg) v = (j < L0.cap && j0 == 0) ? pa0[p] : (j < L0.cap && j0 == 32) ? pa1[p] : L0.adj[base + j];
+                    bool fresh = false;
+                    if (v >= 0 && v < lim0) {
+                        int32_t *slot = tab + (((uint32_t)v * 2654435769u) >> hshift);
+                        if (*slot != v) {
+                            *slot = v;
+                            fresh = true;
+                        }
+                    }
+                    if (!append_pending(fresh, v, v, crow, cid, n, rb, lane, flush0)) {
+                        failed = true;
+                        break;
+                    }
+                }
+            }
+            if (!failed && n > 0 && !flush0(n)) failed = true;
+        }
+        if (failed) {
+            if (lane == 0) atomicExch(a.work + 1, 1);
+            return;
+        }
+
+        int32_t *out = a.cand + q * a.cand_stride;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            const int i = lane * S + s;
+            if (i < L) out[i] = list.d[s] < kInf ? (int32_t)(list.id[s] & ~kExpanded) : -1;
+        }
+        if (a.counters && lane == 0) {
+            int32_t *cp = a.counters + q * 6;
+#pragma unroll
+            for (int i = 0; i < 6; i++) cp[i] = cnt[i];
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- rerank ---
+// Bitonic sort of n (power of two) entries in shared memory by (distance, id).
 __device__ __forceinline__ void smem_sort(float *d, uint32_t *id, int n, int lane) {
     for (int size = 2; size <= n; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
@@ -218,7 +633,7 @@ __device__ __forceinline__ void smem_sort(float *d, uint32_t *id, int n, int lan
                 const bool up = (lo & size) == 0;
                 const float dl = d[lo], dh = d[hi];
                 const uint32_t il = id[lo], ih = id[hi];
-                const bool swap = up ? ent_less(dh, ih, dl, il) : ent_less(dl, il, dh, ih);
+                const bool swap = up ? key_less(dh, ih, dl, il) : key_less(dl, il, dh, ih);
                 if (swap) {
                     d[lo] = dh;
                     d[hi] = dl;
@@ -231,305 +646,110 @@ __device__ __forceinline__ void smem_sort(float *d, uint32_t *id, int n, int lan
     }
 }
 
-template <int DT, int KMAX, int TRAV, int KT>
-__global__ void __launch_bounds__(128, 6)
-    search_fast_kernel(const DevGraph *__restrict__ gp, const LaneCfg lc, const TravCfg tc, const FastArgs a) {
+template <int DT, int KMAX>
+__global__ void __launch_bounds__(128)
+    rerank_kernel(const DevGraph *__restrict__ gp, const LaneCfg lc, const RerankArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
-    const int64_t gwarp = (int64_t)blockIdx.x * wpb + wib;
-    const int Lmax = a.list_cap;
-    unsigned char *my = smem + (size_t)wib * fast_smem_per_warp(Lmax, a.rowbuf_bytes);
-    ListBuf A{reinterpret_cast<float *>(my), reinterpret_cast<uint32_t *>(my) + Lmax};
-    ListBuf B{reinterpret_cast<float *>(my) + 2 * Lmax, reinterpret_cast<uint32_t *>(my) + 3 * Lmax};
-    float *newd = reinterpret_cast<float *>(my) + 4 * Lmax;
-    uint32_t *newid = reinterpret_cast<uint32_t *>(newd + 32);
-    Stage *st = reinterpret_cast<Stage *>(newid + 32);
-    uint8_t *rowbuf = reinterpret_cast<uint8_t *>(st + 1);
-
-    WarpScratch ws;
-    ws.st = st;
-    ws.rowbuf = rowbuf;
-    ws.bind(a.gs, gwarp);
-
+    const RerankLayout lay = rerank_layout(a.cand_stride, a.row_bytes);
+    unsigned char *my = smem + (size_t)wib * lay.total;
+    Stage *st = reinterpret_cast<Stage *>(my);
+    float *sd = reinterpret_cast<float *>(my + lay.sd);
+    uint32_t *sid = reinterpret_cast<uint32_t *>(my + lay.sid);
+    uint8_t *rowbuf = my + lay.rowbuf;
     const VecView vv{gp->vec0, gp->zero_row, gp->row_bytes};
-    const TravView tv{a.trav, a.trav_zero, a.trav_row_bytes, a.rownorm};
     const bool ip = gp->metric == PK_METRIC_IP;
-    const int enter_level = gp->enter_level;
-    const DevLayer L0 = gp->L[0];
-
-    for (;;) {
-        int qi = 0;
-        if (lane == 0) qi = atomicAdd(a.work, 1);
-        qi = __shfl_sync(kFull, qi, 0);
-        if (qi >= a.nq) break;
-        const int q = qi;
+    const bool walk_failed = *a.status != 0;
+    for (int64_t q = (int64_t)blockIdx.x * wpb + wib; q < a.nq; q += (int64_t)gridDim.x * wpb) {
         const int k = max(0, min(a.k_arr ? a.k_arr[q] : a.k, a.out_stride));
-        const int ef = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, Lmax));
-        const int L = ef;
-
-        // traversal query: lane-local chunks of the query in the traversal format
-        TravQuery<TRAV, KT> tq;
-        float qnorm = 0.f;
-        {
-            const int G = tc.GT, gl = lane % G;
-            const uint8_t *qrow = a.tq_rows + (int64_t)q * a.tq_row_bytes;
-#pragma unroll
-            for (int kk = 0; kk < KT; kk++) {
-                const int c = gl + kk * G;
-                if constexpr (TRAV == kTravF16) {
-                    tq.q[kk] = c < tc.CT ? ld16(qrow + c * 16) : make_uint4(0, 0, 0, 0);
-                } else {
-#pragma unroll
-                    for (int e = 0; e < 16; e++) tq.q[kk][e] = 0.f;
-                    if (c < tc.CT) {
-                        const float *qf = reinterpret_cast<const float *>(qrow) + c * 16;
-#pragma unroll
-                        for (int e = 0; e < 16; e++) tq.q[kk][e] = qf[e];
-                    }
-                }
+        const int L = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, a.cand_stride));
+        int32_t *oid = a.out_ids + q * a.out_stride;
+        float *od = a.out_dists + q * a.out_stride;
+        if (walk_failed) {
+            // no result rather than a stale one
+            for (int i = lane; i < k; i += 32) {
+                oid[i] = -1;
+                od[i] = FLT_MAX;
             }
-            if (TRAV == kTravE4M3) qnorm = a.qnorm[q];
+            continue;
         }
-
-        int32_t cnt[6] = {0, 0, 0, 0, 0, 0};
-        // ---- upper layers: greedy descent with traversal distances ----
-        int32_t enter = gp->L[enter_level].ent;
-        for (int level = enter_level; level >= 1; --level) {
-            const DevLayer Ly = gp->L[level];
-            if (lane == 0) st->row[0] = Ly.vrow[enter];
-            __syncwarp();
-            trav_dist_rows<TRAV, KT>(tv, tc, tq, ip, qnorm, st->row, st->d, 1, rowbuf, lane);
-            __syncwarp();
-            float cd = st->d[0];
-            __syncwarp();
-            int32_t c = enter;
-            if (lane == 0) ws.mark_one(enter);
-            ws.vl_n++;
-            __syncwarp();
-            bool updated;
-            int64_t rounds = 0;
-            do {
-                updated = false;
-                const int32_t cur = c;
-                const int64_t base = (int64_t)cur * Ly.cap;
-                const int deg = Ly.deg[cur];
-                cnt[0]++;
-                cnt[2] += deg;
-                for (int j0 = 0; j0 < deg; j0 += 32) {
-                    const int nn = take_new(Ly, false, base, j0, deg, ws, lane, false, 0);
-                    trav_dist_rows<TRAV, KT>(tv, tc, tq, ip, qnorm, st->row, st->d, nn, rowbuf, lane);
-                    __syncwarp();
-                    for (int t = 0; t < nn; t++) {
-                        const float d = st->d[t];
-                        if (d < cd) {
-                            cd = d;
-                            c = st->id[t];
-                            updated = true;
-                        }
-                    }
-                    cnt[1] += nn;
-                    __syncwarp();
-                }
-            } while (updated && ++rounds <= Ly.lcap);
-            ws.end_layer(lane);
-            const int32_t dn = Ly.down[c];
-            enter = dn >= 0 ? dn : gp->L[level - 1].ent;
-        }
-
-        // ---- layer 0: best-first walk over a sorted list of ef slots ----
-        int count = 0;
-        {
-            if (lane == 0) st->row[0] = enter;
-            __syncwarp();
-            trav_dist_rows<TRAV, KT>(tv, tc, tq, ip, qnorm, st->row, st->d, 1, rowbuf, lane);
-            __syncwarp();
-            if (lane == 0) {
-                A.d[0] = st->d[0];
-                A.id[0] = (uint32_t)enter;
-                ws.mark_one(enter);
-            }
-            ws.vl_n++;
-            count = 1;
-            __syncwarp();
-        }
-        int64_t iters = 0;
-        for (;;) {
-            // the P best unexpanded entries, in list order
-            int picked[4] = {-1, -1, -1, -1};
-            int np = 0;
-            for (int base = 0; base < count && np < a.expand; base += 32) {
-                const int i = base + lane;
-                const bool un = i < count && !(A.id[i] & kExpanded);
-                unsigned m = __ballot_sync(kFull, un);
-                while (m && np < a.expand) {
-                    const int b = __ffs(m) - 1;
-                    picked[np++] = base + b;
-                    m &= m - 1;
-                }
-            }
-            if (np == 0 || ++iters > L0.lcap) break;
-            // the ids now: a merge below moves entries to the other buffer
-            int32_t cids[4];
-#pragma unroll
-            for (int p = 0; p < 4; p++) cids[p] = p < np ? (int32_t)(A.id[picked[p]] & ~kExpanded) : -1;
-            __syncwarp();
-            if (lane == 0)
-                for (int p = 0; p < np; p++) A.id[picked[p]] |= kExpanded;
-            __syncwarp();
-            for (int p = 0; p < np; p++) {
-                const int32_t cid = cids[p];
-                const int64_t base = (int64_t)cid * L0.cap;
-                const int32_t pre = lane < L0.cap ? L0.adj[base + lane] : -1;
-                const int deg = L0.deg[cid];
-                cnt[3]++;
-                cnt[5] += deg;
-                for (int j0 = 0; j0 < deg; j0 += 32) {
-                    const int nn = take_new(L0, true, base, j0, deg, ws, lane, j0 == 0 && L0.cap >= 32, pre);
-                    cnt[4] += nn;
-                    if (nn == 0) continue;
-                    trav_dist_rows<TRAV, KT>(tv, tc, tq, ip, qnorm, st->row, st->d, nn, rowbuf, lane);
-                    __syncwarp();
-                    // keep what beats the worst listed entry once the list is full
-                    float nd = FLT_MAX;
-                    uint32_t nid = 0x7fffffffu;
-                    if (lane < nn) {
-                        nd = st->d[lane];
-                        nid = (uint32_t)st->id[lane];
-                        if (count >= L && !ent_less(nd, nid, A.d[count - 1], A.id[count - 1])) {
-                            nd = FLT_MAX;
-                            nid = 0x7fffffffu;
-                        }
-                    }
-                    const unsigned keep = __ballot_sync(kFull, nd != FLT_MAX);
-                    const int m = __popc(keep);
-                    if (m == 0) continue;
-                    if (m <= 4) {
-                        // a few survivors: insert each by shifting the list
-                        // tail one slot (lanes own list slots i = lane + 32j)
-                        unsigned left = keep;
-                        while (left) {
-                            const int src = __ffs(left) - 1;
-                            left &= left - 1;
-                            const float cd = __shfl_sync(kFull, nd, src);
-                            const uint32_t ci = __shfl_sync(kFull, nid, src);
-                            if (count >= L && !ent_less(cd, ci, A.d[count - 1], A.id[count - 1])) continue;
-                            int pos = 0;
-                            for (int b = 0; b < count; b += 32) {
-                                const int i = b + lane;
-                                pos += __popc(__ballot_sync(kFull, i < count && ent_less(A.d[i], A.id[i], cd, ci)));
-                            }
-                            const int last = min(count, L - 1);  // slot the tail moves into
-                            // move [pos, last) up by one, from the top down
-                            for (int b = ((last - 1) / 32) * 32; b >= 0 && last > pos; b -= 32) {
-                                const int i = b + lane;
-                                float vd = 0.f;
-                                uint32_t vi = 0;
-                                const bool mv = i >= pos && i < last;
-                                if (mv) {
-                                    vd = A.d[i];
-                                    vi = A.id[i];
-                                }
-                                __syncwarp();
-                                if (mv) {
-                                    A.d[i + 1] = vd;
-                                    A.id[i + 1] = vi;
-                                }
-                                __syncwarp();
-                            }
-                            if (lane == 0) {
-                                A.d[pos] = cd;
-                                A.id[pos] = ci;
-                            }
-                            count = min(count + 1, L);
-                            __syncwarp();
-                        }
-                    } else {
-                        warp_sort32(nd, nid, lane);
-                        count = merge_into(A, B, count, L, nd, nid, m, newd, newid, lane);
-                        const ListBuf T = A;
-                        A = B;
-                        B = T;
-                    }
-                }
-            }
-        }
-        ws.end_layer(lane);
-
-        // ---- re-rank the listed entries with exact distances ----
         uint4 qr[KMAX];
-        load_regs<KMAX>(qr, a.queries + (int64_t)q * vv.row_bytes, lc, lane, false);
-        const int R = count;
-        for (int b0 = 0; b0 < R; b0 += 32) {
-            const int nn = min(32, R - b0);
-            if (lane < nn) st->row[lane] = (int32_t)(A.id[b0 + lane] & ~kExpanded);
+        load_regs<KMAX>(qr, a.queries + q * vv.row_bytes, lc, lane, false);
+        const int32_t *cl = a.cand + q * a.cand_stride;
+        for (int b0 = 0; b0 < L; b0 += 32) {
+            const int nn = min(32, L - b0);
+            int32_t r = -1;
+            if (lane < nn) {
+                r = cl[b0 + lane];
+                st->row[lane] = r;
+            }
             __syncwarp();
             dist_rows_staged<DT, KMAX>(vv, lc, qr, ip, st->row, st->d, nn, rowbuf, lane);
             __syncwarp();
             if (lane < nn) {
-                B.d[b0 + lane] = st->d[lane];
-                B.id[b0 + lane] = A.id[b0 + lane] & ~kExpanded;
+                sd[b0 + lane] = r >= 0 ? st->d[lane] : FLT_MAX;
+                sid[b0 + lane] = r >= 0 ? (uint32_t)r : 0x7fffffffu;
             }
             __syncwarp();
         }
         int n2 = 1;
-        while (n2 < R) n2 <<= 1;
-        for (int i = R + lane; i < n2; i += 32) {
-            B.d[i] = FLT_MAX;
-            B.id[i] = 0x7fffffffu;
+        while (n2 < L) n2 <<= 1;
+        for (int i = L + lane; i < n2; i += 32) {
+            sd[i] = FLT_MAX;
+            sid[i] = 0x7fffffffu;
         }
         __syncwarp();
-        smem_sort(B.d, B.id, n2, lane);
-        int32_t *oid = a.out_ids + (int64_t)q * a.out_stride;
-        float *od = a.out_dists + (int64_t)q * a.out_stride;
+        smem_sort(sd, sid, n2, lane);
         for (int i = lane; i < k; i += 32) {
-            if (i < R) {
-                oid[i] = a.ext0[B.id[i]];
-                od[i] = B.d[i];
-            } else {
-                oid[i] = -1;
-                od[i] = FLT_MAX;
-            }
-        }
-        if (a.counters && lane == 0) {
-            int32_t *cp = a.counters + (int64_t)q * 6;
-#pragma unroll
-            for (int i = 0; i < 6; i++) cp[i] = cnt[i];
+            const bool have = i < L && sid[i] != 0x7fffffffu;
+            oid[i] = have ? a.ext0[sid[i]] : -1;
+            od[i] = have ? sd[i] : FLT_MAX;
         }
         __syncwarp();
     }
 }
 
-template <int DT, int KMAX, int TRAV>
-void *pick_kt(int kt) {
+// ------------------------------------------------------------ dispatch -----
+template <int TRAV, int KT>
+void *walk_pick_s(int s) {
+    switch (s) {
+        case 1: return (void *)walk_kernel<TRAV, KT, 1>;
+        case 2: return (void *)walk_kernel<TRAV, KT, 2>;
+        case 4: return (void *)walk_kernel<TRAV, KT, 4>;
+        case 8: return (void *)walk_kernel<TRAV, KT, 8>;
+        case 16: return (void *)walk_kernel<TRAV, KT, 16>;
+        default: return nullptr;
+    }
+}
+void *walk_kernel_ptr(int trav, int kt, int s) {
+    if (trav == kTravF16) return kt == 1 ? walk_pick_s<kTravF16, 1>(s) : nullptr;
+    if (trav != kTravE4M3) return nullptr;
     switch (kt) {
-        case 1: return (void *)search_fast_kernel<DT, KMAX, TRAV, 1>;
-        case 2: return (void *)search_fast_kernel<DT, KMAX, TRAV, 2>;
-        case 4: return (void *)search_fast_kernel<DT, KMAX, TRAV, 4>;
+        case 1: return walk_pick_s<kTravE4M3, 1>(s);
+        case 2: return walk_pick_s<kTravE4M3, 2>(s);
+        case 4: return walk_pick_s<kTravE4M3, 4>(s);
         default: return nullptr;
     }
 }
-template <int DT, int KMAX>
-void *pick_trav(int trav, int kt) {
-    return trav == kTravF16 ? pick_kt<DT, KMAX, kTravF16>(kt) : pick_kt<DT, KMAX, kTravE4M3>(kt);
-}
+
 template <int DT>
-void *pick_kmax(int kmax, int trav, int kt) {
+void *rerank_pick(int kmax) {
     switch (kmax) {
-        case 1: return pick_trav<DT, 1>(trav, kt);
-        case 2: return pick_trav<DT, 2>(trav, kt);
-        case 4: return pick_trav<DT, 4>(trav, kt);
-        case 8: return pick_trav<DT, 8>(trav, kt);
+        case 1: return (void *)rerank_kernel<DT, 1>;
+        case 2: return (void *)rerank_kernel<DT, 2>;
+        case 4: return (void *)rerank_kernel<DT, 4>;
+        case 8: return (void *)rerank_kernel<DT, 8>;
         default: return nullptr;
     }
 }
-void *fast_kernel_ptr(int dtype, int kmax, int trav, int kt) {
+void *rerank_kernel_ptr(int dtype, int kmax) {
     switch (dtype) {
-        case PK_DTYPE_U8: return pick_kmax<PK_DTYPE_U8>(kmax, trav, kt);
-        case PK_DTYPE_I8: return pick_kmax<PK_DTYPE_I8>(kmax, trav, kt);
-        case PK_DTYPE_F32: return pick_kmax<PK_DTYPE_F32>(kmax, trav, kt);
-        case PK_DTYPE_F16: return pick_kmax<PK_DTYPE_F16>(kmax, trav, kt);
+        case PK_DTYPE_U8: return rerank_pick<PK_DTYPE_U8>(kmax);
+        case PK_DTYPE_I8: return rerank_pick<PK_DTYPE_I8>(kmax);
+        case PK_DTYPE_F32: return rerank_pick<PK_DTYPE_F32>(kmax);
+        case PK_DTYPE_F16: return rerank_pick<PK_DTYPE_F16>(kmax);
         default: return nullptr;
     }
 }
@@ -561,8 +781,8 @@ __device__ __forceinline__ float elem(const uint8_t *row, int d) {
     return (float)reinterpret_cast<const int8_t *>(row)[d];
 }
 
-// Rows [r0, r1) of vec0 into the traversal copy (and, for E4M3, the per-row
-// norm of the scaled stored values).  One block per row.
+// Rows [r0, r1) of vec0 into the traversal copy (divided by the scales) and
+// the per-row sum of squares of the stored values.  One block per row.
 template <int DT, int TRAV>
 __global__ void convert_rows_kernel(const uint8_t *vec0, int64_t row_bytes, int64_t r0, int64_t r1, int dim,
                                     const float *scale, uint8_t *trav, int64_t trav_row_bytes, float *rownorm) {
@@ -573,32 +793,35 @@ __global__ void convert_rows_kernel(const uint8_t *vec0, int64_t row_bytes, int6
         float part = 0.f;
         for (int d = threadIdx.x; d < dim; d += blockDim.x) {
             const float v = elem<DT>(row, d);
+            float back;
             if constexpr (TRAV == kTravF16) {
-                reinterpret_cast<__half *>(out)[d] = __float2half_rn(v);
+                const __half h = __float2half_rn(v / scale[d]);
+                reinterpret_cast<__half *>(out)[d] = h;
+                back = __half2float(h);
             } else {
                 const __nv_fp8_storage_t x = __nv_cvt_float_to_fp8(v / scale[d], __NV_SATFINITE, __NV_E4M3);
                 out[d] = x;
-                const float back = __half2float(__half(__nv_cvt_fp8_to_halfraw(x, __NV_E4M3))) * scale[d];
-                part += back * back;
+                back = __half2float(__half(__nv_cvt_fp8_to_halfraw(x, __NV_E4M3))) * scale[d];
             }
+            part += back * back;
         }
-        if (TRAV == kTravE4M3) {
-            for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(kFull, part, off);
-            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                float s = 0.f;
-                for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
-                rownorm[r] = s;
-            }
-            __syncthreads();
+        for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(kFull, part, off);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float sum = 0.f;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += red[w];
+            rownorm[r] = sum;
         }
+        __syncthreads();
     }
 }
 
-// Queries into the traversal format: F16 rows of halves (padded), or E4M3
-// rows of floats pre-multiplied by the per-dimension scales (padded to a
-// multiple of 16 elements) plus sum_d q_d^2 for L2.
+// Queries into the traversal format.  FP16: rows of halves divided by the
+// scale (clamped to 64 scaled units: the copy's rows stay within 32), zero
+// padded, plus the sum of squares of the stored halves.  E4M3: rows of floats
+// pre-multiplied by the per-dimension scales (padded to a multiple of 16
+// elements) plus sum_d q_d^2.
 template <int DT, int TRAV>
 __global__ void prep_queries_kernel(const uint8_t *q, int64_t row_bytes, int64_t nq, int dim, const float *scale,
                                     uint8_t *out, int64_t out_row_bytes, float *qnorm) {
@@ -611,23 +834,24 @@ __global__ void prep_queries_kernel(const uint8_t *q, int64_t row_bytes, int64_t
         for (int d = threadIdx.x; d < padded; d += blockDim.x) {
             const float v = d < dim ? elem<DT>(row, d) : 0.f;
             if constexpr (TRAV == kTravF16) {
-                reinterpret_cast<__half *>(o)[d] = __float2half_rn(v);
+                const __half h = __float2half_rn(d < dim ? fminf(fmaxf(v / scale[d], -64.f), 64.f) : 0.f);
+                reinterpret_cast<__half *>(o)[d] = h;
+                const float b = __half2float(h);
+                part += b * b;
             } else {
                 reinterpret_cast<float *>(o)[d] = d < dim ? v * scale[d] : 0.f;
                 part += v * v;
             }
         }
-        if (TRAV == kTravE4M3) {
-            for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(kFull, part, off);
-            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                float s = 0.f;
-                for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
-                qnorm[r] = s;
-            }
-            __syncthreads();
+        for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(kFull, part, off);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float sum = 0.f;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += red[w];
+            qnorm[r] = sum;
         }
+        __syncthreads();
     }
 }
 
@@ -636,12 +860,17 @@ __global__ void prep_queries_kernel(const uint8_t *q, int64_t row_bytes, int64_t
 TravCfgHost trav_config(int64_t trav_row_bytes, int trav) {
     TravCfgHost t;
     t.CT = (int)(trav_row_bytes / 16);
-    // FP16: groups of G lanes with up to 4 chunks each (as the exact path);
+    if (trav == kTravF16) {
+        // the tensor-core path keeps the query in shared memory
+        t.GT = 32;
+        t.KT = 1;
+        t.KTMAX = 1;
+        return t;
+    }
     // E4M3: a chunk holds 16 elements, whose query part is 16 floats, so a
-    // lane keeps one chunk
-    const int want = trav == kTravF16 ? (t.CT + 3) / 4 : t.CT;
-    int G = trav == kTravF16 ? 2 : 1;
-    while (G < want && G < 32) G *= 2;
+    // lane keeps one chunk; groups of G lanes (a power of two) per row
+    int G = 1;
+    while (G < t.CT && G < 32) G *= 2;
     t.GT = G;
     t.KT = (t.CT + G - 1) / G;
     int kt = 1;
@@ -650,8 +879,8 @@ TravCfgHost trav_config(int64_t trav_row_bytes, int trav) {
     return t;
 }
 
-int fast_blocks_per_sm(int dtype, const LaneCfg &lc, int trav, const TravCfgHost &tc, int wpb, size_t smem) {
-    void *fn = fast_kernel_ptr(dtype, lc.KMAX, trav, tc.KTMAX);
+int walk_blocks_per_sm(int trav, const TravCfgHost &tc, int slots, int wpb, size_t smem) {
+    void *fn = walk_kernel_ptr(trav, tc.KTMAX, slots);
     if (!fn) return 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
@@ -659,14 +888,33 @@ int fast_blocks_per_sm(int dtype, const LaneCfg &lc, int trav, const TravCfgHost
     return nb;
 }
 
-cudaError_t launch_search_fast(const DevGraph *g, int dtype, const LaneCfg &lc, int trav, const TravCfgHost &tch,
-                               const FastArgs &a, int grid, int wpb, size_t smem, cudaStream_t s) {
-    void *fn = fast_kernel_ptr(dtype, lc.KMAX, trav, tch.KTMAX);
+cudaError_t launch_walk(const DevGraph *g, int trav, const TravCfgHost &tch, int slots, const WalkArgs &a, int grid,
+                        int wpb, size_t smem, cudaStream_t s) {
+    void *fn = walk_kernel_ptr(trav, tch.KTMAX, slots);
     if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     TravCfg tc{tch.GT, tch.KT, tch.CT};
-    void *args[] = {(void *)&g, (void *)&lc, (void *)&tc, (void *)&a};
+    void *args[] = {(void *)&g, (void *)&tc, (void *)&a};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(wpb * 32), args, smem, s);
+}
+
+int rerank_blocks_per_sm(int dtype, const LaneCfg &lc, int wpb, size_t smem) {
+    void *fn = rerank_kernel_ptr(dtype, lc.KMAX);
+    if (!fn) return 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, wpb * 32, smem) != cudaSuccess) return 0;
+    return nb;
+}
+
+cudaError_t launch_rerank(const DevGraph *g, int dtype, const LaneCfg &lc, const RerankArgs &a, int grid, int wpb,
+                          size_t smem, cudaStream_t s) {
+    void *fn = rerank_kernel_ptr(dtype, lc.KMAX);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    void *args[] = {(void *)&g, (void *)&lc, (void *)&a};
     return cudaLaunchKernel(fn, dim3(grid), dim3(wpb * 32), args, smem, s);
 }
 

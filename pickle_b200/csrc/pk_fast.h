@@ -8,44 +8,101 @@ namespace pk {
 constexpr int kTravF16 = 1;   // traversal copy in FP16
 constexpr int kTravE4M3 = 2;  // traversal copy in FP8 E4M3 with per-dimension scales
 
+constexpr int kFastMaxEf = 512;  // the walk's register list holds up to 32 * 16 entries
+
 struct TravCfgHost {
     int GT, KT, CT, KTMAX;
 };
 TravCfgHost trav_config(int64_t trav_row_bytes, int trav);
 
-struct FastArgs {
+// Walk launch parameters.
+struct WalkArgs {
     int64_t nq;
-    int32_t k, ef;                 // uniform values (ef also bounds ef_arr)
+    int32_t ef;                 // uniform ef, or the bound of ef_arr
+    int32_t expand;             // list entries expanded per iteration (1..4)
+    const int32_t *ef_arr;
+    int32_t *counters;          // nq * 6 or null
+    int32_t *work;              // [0] query counter, [1] status: 1 = a row fetch timed out
+    int32_t *cand;              // nq * cand_stride: each query's final list (ids, -1 = empty)
+    int32_t cand_stride;        // 32 * list slots per lane
+    int32_t rb;                 // rows per fetch batch
+    int32_t hlog2;              // log2 of the visited-filter slots
+    int32_t pad_;
+    const uint8_t *tq_rows;     // traversal queries
+    int64_t tq_row_bytes;
+    const float *qnorm;         // sum of squares of each traversal query (L2)
+    const uint8_t *trav;        // traversal copy of the vectors
+    const uint8_t *trav_zero;   // a zero row of the traversal copy
+    int64_t trav_row_bytes;
+    int64_t trav_rows;          // rows in the traversal copy; node ids stay below it
+    const float *rownorm;       // sum of squares of each stored row (L2)
+};
+
+// Shared-memory stride of a staged traversal row: the row padded to an odd
+// number of 16-byte chunks, so that 8 consecutive rows start in 8 different
+// groups of banks (conflict-free ldmatrix and 16-byte loads).
+__host__ __device__ inline int64_t stage_stride(int64_t trav_row_bytes) {
+    return ((trav_row_bytes / 16) & 1) ? trav_row_bytes : trav_row_bytes + 16;
+}
+
+// Shared memory of one walk warp: the staged rows (rb rows, stride apart),
+// the query in the traversal format, the visited filter, the pending batch
+// (rows, ids, distances), the mbarrier.  Every region starts on a 16-byte
+// boundary (bulk copies land on 16-byte boundaries).
+struct WalkLayout {
+    int rowbuf, qbuf, tab, crow, cid, cd, bar, total;
+    int64_t stride;
+};
+__host__ __device__ inline WalkLayout walk_layout(int rb, int64_t trav_row_bytes, int hlog2) {
+    WalkLayout w;
+    w.stride = stage_stride(trav_row_bytes);
+    w.rowbuf = 0;
+    w.qbuf = align16((int64_t)rb * w.stride);
+    w.tab = w.qbuf + align16(trav_row_bytes);
+    w.crow = w.tab + (4 << hlog2);
+    w.cid = w.crow + align16(4 * (int64_t)rb);
+    w.cd = w.cid + align16(4 * (int64_t)rb);
+    w.bar = w.cd + align16(4 * (int64_t)rb);
+    w.total = w.bar + 16;
+    return w;
+}
+
+// Re-rank launch parameters.
+struct RerankArgs {
+    int64_t nq;
+    int32_t k, ef;              // uniform values (ef also bounds ef_arr)
     const int32_t *k_arr, *ef_arr;
     int32_t out_stride;
+    int32_t cand_stride;
     int32_t *out_ids;
     float *out_dists;
     const int32_t *ext0;
-    int32_t *counters;             // nq * 6 or null
-    int32_t *work;                 // [0] query counter
-    WarpGlobalScratch gs;          // visited bitmaps and id lists
-    int32_t list_cap;              // a power of two >= every ef
-    int32_t rowbuf_bytes;          // kStageRows * max(row_bytes, trav_row_bytes)
-    int32_t expand;                // entries expanded per iteration (1..4)
-    const uint8_t *queries;        // exact queries, padded rows of row_bytes
-    const uint8_t *tq_rows;        // traversal queries
-    int64_t tq_row_bytes;
-    const float *qnorm;            // E4M3: sum of squares of each query
-    const uint8_t *trav;           // traversal copy of the vectors
-    const uint8_t *trav_zero;      // a zero row of the traversal copy
-    int64_t trav_row_bytes;
-    const float *rownorm;          // E4M3: per-row norm of the stored copy
+    const int32_t *cand;
+    const int32_t *status;      // the walk's status: nonzero = its lists are incomplete
+    const uint8_t *queries;     // exact queries, padded rows of row_bytes
+    int64_t row_bytes;
 };
 
-// Shared memory of one warp: two lists of list_cap (distance, id) entries, 32
-// staged new entries, a Stage block, and the row buffer.
-__host__ __device__ inline int fast_smem_per_warp(int list_cap, int rowbuf_bytes) {
-    return align16((int64_t)16 * list_cap + 256 + kStageBytes) + align16(rowbuf_bytes);
+// Shared memory of one re-rank warp: a Stage block, the sort buffers
+// (cand_stride distances and ids), kStageRows exact rows.
+struct RerankLayout {
+    int sd, sid, rowbuf, total;
+};
+__host__ __device__ inline RerankLayout rerank_layout(int cand_stride, int64_t row_bytes) {
+    RerankLayout r;
+    r.sd = kStageBytes;
+    r.sid = r.sd + align16(4 * (int64_t)cand_stride);
+    r.rowbuf = r.sid + align16(4 * (int64_t)cand_stride);
+    r.total = align16(r.rowbuf + kStageRows * row_bytes);
+    return r;
 }
 
-int fast_blocks_per_sm(int dtype, const LaneCfg &lc, int trav, const TravCfgHost &tc, int wpb, size_t smem);
-cudaError_t launch_search_fast(const DevGraph *g, int dtype, const LaneCfg &lc, int trav, const TravCfgHost &tc,
-                               const FastArgs &a, int grid, int wpb, size_t smem, cudaStream_t s);
+int walk_blocks_per_sm(int trav, const TravCfgHost &tc, int slots, int wpb, size_t smem);
+cudaError_t launch_walk(const DevGraph *g, int trav, const TravCfgHost &tc, int slots, const WalkArgs &a, int grid,
+                        int wpb, size_t smem, cudaStream_t s);
+int rerank_blocks_per_sm(int dtype, const LaneCfg &lc, int wpb, size_t smem);
+cudaError_t launch_rerank(const DevGraph *g, int dtype, const LaneCfg &lc, const RerankArgs &a, int grid, int wpb,
+                          size_t smem, cudaStream_t s);
 cudaError_t launch_absmax(int dtype, const uint8_t *vec0, int64_t row_bytes, int64_t n, int dim, uint32_t *out,
                           cudaStream_t s);
 cudaError_t launch_convert_rows(int dtype, int trav, const uint8_t *vec0, int64_t row_bytes, int64_t r0, int64_t r1,

@@ -110,7 +110,10 @@ struct SearchScratch {
 // Per-launch working set of the fast search: scratch and query staging.  The
 // handle owns one; each serving slot owns its own, so slots can overlap.
 struct FastCtx {
-    SearchScratch fs;
+    int32_t *d_work = nullptr;     // [0] query counter of the walk, [1] its status
+    int64_t work_n = 0;
+    int32_t *d_cand = nullptr;     // the walk's final lists, nq * 32 * slots ids
+    int64_t cand_n = 0;
     uint8_t *d_fq = nullptr, *d_tq = nullptr;
     int64_t fq_n = 0, tq_n = 0;
     float *d_qn = nullptr;
@@ -158,10 +161,14 @@ struct pk_index {
     int64_t trav_row_bytes = 0, trav_rows = 0, trav_cap = 0;
     uint8_t *d_trav = nullptr, *d_trav_zero = nullptr;
     float *d_scale = nullptr, *d_rownorm = nullptr;
+    float trav_f16_scale = 1.0f;   // FP16 copy = vectors / this power of two
     FastCtx fctx;
     int32_t *d_fids = nullptr;
     float *d_fdists = nullptr;
     int64_t fids_n = 0, fdists_n = 0;
+    // walk launch shape (0 = the default): rows per fetch batch, log2 of the
+    // visited-filter slots, warps per block
+    int fast_rb = 0, fast_hlog2 = 0, fast_wpb = 0;
 
     size_t dev_bytes = 0;
 
@@ -700,11 +707,42 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
 
 // ------------------------------------------------------------ fast path -----
 
-// (Re)builds the traversal copy of rows [0, n0): per-dimension scales from
-// the rows present now (FP8), then every row converted.
+// Per-dimension largest magnitude of rows [r0, r1) of the vectors.
+int rows_absmax(pk_index *h, int64_t r0, int64_t r1, std::vector<float> &m) {
+    cudaStream_t s = h->stream;
+    m.assign(h->dim, 0.f);
+    if (r1 <= r0) return PK_OK;
+    uint32_t *amax = nullptr;
+    PK_TRY(dalloc(h, (void **)&amax, 4 * (size_t)h->dim));
+    PK_CUDA(cudaMemsetAsync(amax, 0, 4 * (size_t)h->dim, s));
+    PK_CUDA(pk::launch_absmax(h->dtype, h->hg.vec0 + r0 * h->row_bytes, h->row_bytes, r1 - r0, (int)h->dim, amax,
+                              s));
+    PK_CUDA(cudaMemcpyAsync(m.data(), amax, 4 * (size_t)h->dim, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    dfree(h, amax, 4 * (size_t)h->dim);
+    return PK_OK;
+}
+
+// FP16 traversal scale: the power of two sc with max|x| / sc in [4, 8), so
+// that half-precision products and squares stay far inside FP16's range (1
+// for an all-zero or non-finite maximum).
+float f16_scale(const std::vector<float> &m) {
+    float mx = 0.f;
+    for (float v : m) mx = std::max(mx, v);
+    if (!(mx > 0.f) || !std::isfinite(mx)) return 1.0f;
+    int e = 0;
+    std::frexp(mx / 8.0f, &e);  // mx / 8 = f * 2^e with f in [0.5, 1)
+    return std::ldexp(1.0f, e);
+}
+
+// (Re)builds the traversal copy of rows [0, n0): scales from the rows present
+// now (per dimension for FP8, one power of two for FP16), then every row
+// converted, with its stored norm.
 int build_traversal(pk_index *h, int trav) {
     cudaStream_t s = h->stream;
-    const int64_t trb = trav == pk::kTravF16 ? pk::align16(h->dim * 2) : pk::align16(h->dim);
+    // FP16 rows are padded with zeros to whole 16-element steps of the
+    // tensor-core dot products (32 bytes)
+    const int64_t trb = trav == pk::kTravF16 ? (h->dim * 2 + 31) / 32 * 32 : pk::align16(h->dim);
     const int64_t rows = std::max<int64_t>(h->vec_rows, 1);
     PK_CUDA(cudaStreamSynchronize(s));
     dfree(h, h->d_trav, (size_t)(h->trav_cap * h->trav_row_bytes));
@@ -720,19 +758,16 @@ int build_traversal(pk_index *h, int trav) {
     PK_CUDA(cudaMemsetAsync(h->d_trav, 0, (size_t)(rows * trb), s));
     PK_CUDA(cudaMemsetAsync(h->d_trav_zero, 0, (size_t)trb, s));
     PK_CUDA(cudaMemsetAsync(h->d_rownorm, 0, 4 * (size_t)rows, s));
-    std::vector<float> scale(h->dim, 1.0f);
-    if (trav == pk::kTravE4M3 && h->n0() > 0) {
-        uint32_t *amax = nullptr;
-        PK_TRY(dalloc(h, (void **)&amax, 4 * (size_t)h->dim));
-        PK_CUDA(cudaMemsetAsync(amax, 0, 4 * (size_t)h->dim, s));
-        PK_CUDA(pk::launch_absmax(h->dtype, h->hg.vec0, h->row_bytes, h->n0(), (int)h->dim, amax, s));
-        std::vector<float> m(h->dim);
-        PK_CUDA(cudaMemcpyAsync(m.data(), amax, 4 * (size_t)h->dim, cudaMemcpyDeviceToHost, s));
-        PK_CUDA(cudaStreamSynchronize(s));
-        dfree(h, amax, 4 * (size_t)h->dim);
+    std::vector<float> m, scale(h->dim, 1.0f);
+    PK_TRY(rows_absmax(h, 0, h->n0(), m));
+    if (trav == pk::kTravE4M3) {
         // E4M3's largest finite value is 448: map each dimension's largest
         // magnitude onto it
         for (int64_t d = 0; d < h->dim; d++) scale[d] = m[d] > 0.f ? m[d] / 448.0f : 1.0f;
+    } else {
+        const float sc = f16_scale(m);
+        for (int64_t d = 0; d < h->dim; d++) scale[d] = sc;
+        h->trav_f16_scale = sc;
     }
     PK_CUDA(cudaMemcpyAsync(h->d_scale, scale.data(), 4 * (size_t)h->dim, cudaMemcpyHostToDevice, s));
     PK_CUDA(pk::launch_convert_rows(h->dtype, trav, h->hg.vec0, h->row_bytes, 0, h->n0(), (int)h->dim, h->d_scale,
@@ -745,10 +780,19 @@ int build_traversal(pk_index *h, int trav) {
     return PK_OK;
 }
 
-// Rows inserted since the copy was built are converted with the same scales.
+// Rows inserted since the copy was built are converted with the same scales,
+// unless (FP16) they reach past 32 in scaled units, where half-precision
+// squares could overflow: then the copy is rebuilt with a new scale.
 int refresh_traversal(pk_index *h) {
     if (h->trav_rows == h->n0()) return PK_OK;
     if (h->vec_rows > h->trav_cap) return build_traversal(h, h->trav);
+    if (h->trav == pk::kTravF16) {
+        std::vector<float> m;
+        PK_TRY(rows_absmax(h, h->trav_rows, h->n0(), m));
+        float mx = 0.f;
+        for (float v : m) mx = std::max(mx, v);
+        if (!(mx <= 32.0f * h->trav_f16_scale)) return build_traversal(h, h->trav);
+    }
     PK_CUDA(pk::launch_convert_rows(h->dtype, h->trav, h->hg.vec0, h->row_bytes, h->trav_rows, h->n0(), (int)h->dim,
                                     h->d_scale, h->d_trav, h->trav_row_bytes, h->d_rownorm, h->stream));
     PK_CUDA(cudaStreamSynchronize(h->stream));
@@ -756,26 +800,45 @@ int refresh_traversal(pk_index *h) {
     return PK_OK;
 }
 
+// Shape of the walk launch for this index: rows per fetch batch, visited
+// filter size, warps per block, and the shared memory that takes.
+struct WalkShape {
+    int rb, hlog2, wpb;
+    size_t smem;
+};
+int walk_shape(const pk_index *h, WalkShape &w) {
+    const int64_t trb = h->trav_row_bytes;
+    w.rb = h->fast_rb > 0 ? h->fast_rb : (int)std::max<int64_t>(8, std::min<int64_t>(32, 12288 / trb));
+    w.hlog2 = h->fast_hlog2 > 0 ? h->fast_hlog2 : 10;
+    w.wpb = h->fast_wpb > 0 ? h->fast_wpb : 4;
+    w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2).total;
+    while (w.wpb > 1 && w.smem > 200 * 1024) {
+        w.wpb /= 2;
+        w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2).total;
+    }
+    if (w.smem > 227 * 1024) return fail(PK_ERR_ARG, "walk working set exceeds shared memory: lower rows or filter bits");
+    return PK_OK;
+}
+
+// Low-precision walk, then exact re-rank of each query's final list.  Fully
+// asynchronous on stream s.
 int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_queries, int64_t nq, int32_t k,
                     int32_t ef, const int32_t *k_arr, const int32_t *ef_arr, int32_t stride, int32_t *ids,
                     float *dists, int32_t *counters, int32_t expand, cudaStream_t s) {
     if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
+    if (ef > pk::kFastMaxEf) return fail(PK_ERR_ARG, "ef too large for the fast path (max 512)");
     PK_TRY(refresh_traversal(h));
-    const int list_cap = (int)pow2ceil(std::max(32, ef));
-    if (list_cap > 4096) return fail(PK_ERR_ARG, "ef too large for the fast path (max 4096)");
-    const int rowbuf = (int)(pk::kStageRows * std::max(h->row_bytes, h->trav_row_bytes));
-    int wpb = 4;
-    size_t smem = (size_t)wpb * pk::fast_smem_per_warp(list_cap, rowbuf);
-    while (wpb > 1 && smem > 200 * 1024) {
-        wpb /= 2;
-        smem = (size_t)wpb * pk::fast_smem_per_warp(list_cap, rowbuf);
-    }
+    int slots = 1;
+    while (32 * slots < ef) slots *= 2;
+    const int cs = 32 * slots;
+    WalkShape ws;
+    PK_TRY(walk_shape(h, ws));
     const pk::TravCfgHost tc = pk::trav_config(h->trav_row_bytes, h->trav);
-    const int nb = pk::fast_blocks_per_sm(h->dtype, h->lc, h->trav, tc, wpb, smem);
-    if (nb <= 0) return fail(PK_ERR_CUDA, "fast search kernel cannot be resident");
-    const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + wpb - 1) / wpb);
-    const int64_t bm_words = (h->hg.L[0].lcap + 31) / 32 + 1;
-    PK_TRY(ensure_scratch(h, c.fs, grid * wpb, bm_words, std::max<int64_t>(8192, 64LL * ef), 1));
+    const int nb = pk::walk_blocks_per_sm(h->trav, tc, slots, ws.wpb, ws.smem);
+    if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
+    const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + ws.wpb - 1) / ws.wpb);
+    PK_TRY(ensure_buf(h, &c.d_work, c.work_n, 2));
+    PK_TRY(ensure_buf(h, &c.d_cand, c.cand_n, nq * cs));
     // exact queries (padded rows) and traversal queries
     const size_t w = (size_t)(h->dim * h->esz);
     const uint8_t *qx = static_cast<const uint8_t *>(queries);
@@ -791,32 +854,62 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     PK_TRY(ensure_buf(h, &c.d_qn, c.qn_n, nq));
     PK_CUDA(pk::launch_prep_queries(h->dtype, h->trav, qx, h->row_bytes, nq, (int)h->dim, h->d_scale, c.d_tq, tq_rb,
                                     c.d_qn, s));
-    PK_CUDA(cudaMemsetAsync(c.fs.work, 0, sizeof(int32_t) * 2, s));
-    pk::FastArgs a{};
+    PK_CUDA(cudaMemsetAsync(c.d_work, 0, sizeof(int32_t) * 2, s));
+    pk::WalkArgs a{};
     a.nq = nq;
-    a.k = k;
     a.ef = ef;
-    a.k_arr = k_arr;
-    a.ef_arr = ef_arr;
-    a.out_stride = stride;
-    a.out_ids = ids;
-    a.out_dists = dists;
-    a.ext0 = h->hg.L[0].ext;
-    a.counters = counters;
-    a.work = c.fs.work;
-    a.gs = c.fs.view();
-    a.list_cap = list_cap;
-    a.rowbuf_bytes = rowbuf;
     a.expand = std::max(1, std::min(4, expand > 0 ? expand : 1));
-    a.queries = qx;
+    a.ef_arr = ef_arr;
+    a.counters = counters;
+    a.work = c.d_work;
+    a.cand = c.d_cand;
+    a.cand_stride = cs;
+    a.rb = ws.rb;
+    a.hlog2 = ws.hlog2;
     a.tq_rows = c.d_tq;
     a.tq_row_bytes = tq_rb;
     a.qnorm = c.d_qn;
     a.trav = h->d_trav;
     a.trav_zero = h->d_trav_zero;
     a.trav_row_bytes = h->trav_row_bytes;
+    a.trav_rows = h->trav_rows;
     a.rownorm = h->d_rownorm;
-    PK_CUDA(pk::launch_search_fast(h->dg, h->dtype, h->lc, h->trav, tc, a, (int)grid, wpb, smem, s));
+    PK_CUDA(pk::launch_walk(h->dg, h->trav, tc, slots, a, (int)grid, ws.wpb, ws.smem, s));
+
+    int rwpb = 4;
+    size_t rsmem = (size_t)rwpb * pk::rerank_layout(cs, h->row_bytes).total;
+    while (rwpb > 1 && rsmem > 200 * 1024) {
+        rwpb /= 2;
+        rsmem = (size_t)rwpb * pk::rerank_layout(cs, h->row_bytes).total;
+    }
+    const int rnb = pk::rerank_blocks_per_sm(h->dtype, h->lc, rwpb, rsmem);
+    if (rnb <= 0) return fail(PK_ERR_CUDA, "re-rank kernel cannot be resident");
+    const int64_t rgrid = std::min<int64_t>((int64_t)rnb * h->num_sms, (nq + rwpb - 1) / rwpb);
+    pk::RerankArgs r{};
+    r.nq = nq;
+    r.k = k;
+    r.ef = ef;
+    r.k_arr = k_arr;
+    r.ef_arr = ef_arr;
+    r.out_stride = stride;
+    r.cand_stride = cs;
+    r.out_ids = ids;
+    r.out_dists = dists;
+    r.ext0 = h->hg.L[0].ext;
+    r.cand = c.d_cand;
+    r.status = c.d_work + 1;
+    r.queries = qx;
+    r.row_bytes = h->row_bytes;
+    PK_CUDA(pk::launch_rerank(h->dg, h->dtype, h->lc, r, (int)rgrid, rwpb, rsmem, s));
+    return PK_OK;
+}
+
+// After a synchronised fast search: the walk's status.
+int fast_status(pk_index *h, FastCtx &c, cudaStream_t s) {
+    int32_t st = 0;
+    PK_CUDA(cudaMemcpyAsync(&st, c.d_work + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    if (st != 0) return fail(PK_ERR_TIMEOUT, "a row fetch of the fast search did not complete in time");
     return PK_OK;
 }
 
@@ -862,7 +955,8 @@ int init_handle(pk_index *h, int metric, int dtype, int64_t dim, int64_t M, int6
 }
 
 void free_fast_ctx(pk_index *h, FastCtx &c) {
-    free_scratch(h, c.fs);
+    dfree(h, c.d_work, 4 * (size_t)c.work_n);
+    dfree(h, c.d_cand, 4 * (size_t)c.cand_n);
     dfree(h, c.d_fq, (size_t)c.fq_n);
     dfree(h, c.d_tq, (size_t)c.tq_n);
     dfree(h, c.d_qn, 4 * (size_t)c.qn_n);
@@ -1262,7 +1356,7 @@ static int pk_index_search_fast_host_impl(pk_index *h, const void *queries, int6
     PK_CUDA(cudaMemcpyAsync(out_ids, h->d_fids, sizeof(int32_t) * nq * k, cudaMemcpyDeviceToHost, s));
     PK_CUDA(cudaMemcpyAsync(out_dists, h->d_fdists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, s));
     PK_CUDA(cudaStreamSynchronize(s));
-    return PK_OK;
+    return fast_status(h, h->fctx, s);
 }
 
 }  // namespace
@@ -1304,6 +1398,7 @@ struct SrvSlot {
     uint8_t *d_q = nullptr;
     int32_t *d_k = nullptr, *d_ef = nullptr, *d_ids = nullptr;
     float *d_d = nullptr;
+    int32_t *h_status = nullptr;   // the walk's status, copied back with the results
     bool busy = false;
     std::vector<std::shared_ptr<SrvRequest>> reqs;
     std::vector<int32_t> offs;
@@ -1376,11 +1471,12 @@ void srv_loop(pk_server *S) {
             const cudaError_t e = cudaEventQuery(sl.ev);
             if (e == cudaErrorNotReady) continue;
             const auto now = Clock::now();
+            const int code = e != cudaSuccess ? PK_ERR_CUDA : *sl.h_status != 0 ? PK_ERR_TIMEOUT : PK_OK;
             std::lock_guard<std::mutex> lk(S->mu);
             for (size_t i = 0; i < sl.reqs.size(); i++) {
                 SrvRequest &r = *sl.reqs[i];
-                if (e != cudaSuccess) {
-                    r.status = PK_ERR_CUDA;
+                if (code != PK_OK) {
+                    r.status = code;
                 } else {
                     r.ids.resize((size_t)r.nq * r.k);
                     r.dists.resize((size_t)r.nq * r.k);
@@ -1393,7 +1489,7 @@ void srv_loop(pk_server *S) {
                 r.done = true;
                 r.t_done = now;
             }
-            if (e != cudaSuccess) srv_fail_all(S, PK_ERR_CUDA);
+            if (code != PK_OK) srv_fail_all(S, code);
             sl.reqs.clear();
             sl.offs.clear();
             sl.busy = false;
@@ -1437,6 +1533,8 @@ void srv_loop(pk_server *S) {
                                      sl.stream) != cudaSuccess ||
                      cudaMemcpyAsync(sl.h_d, sl.d_d, 4 * (size_t)nq * S->max_k, cudaMemcpyDeviceToHost, sl.stream) !=
                          cudaSuccess ||
+                     cudaMemcpyAsync(sl.h_status, sl.ctx.d_work + 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                     sl.stream) != cudaSuccess ||
                      cudaEventRecord(sl.ev, sl.stream) != cudaSuccess))
                     rc = PK_ERR_CUDA;
                 lk.lock();
@@ -1482,6 +1580,7 @@ void srv_free(pk_server *S) {
         cudaFreeHost(sl.h_ef);
         cudaFreeHost(sl.h_ids);
         cudaFreeHost(sl.h_d);
+        cudaFreeHost(sl.h_status);
         cudaFree(sl.d_q);
         cudaFree(sl.d_k);
         cudaFree(sl.d_ef);
@@ -1519,6 +1618,7 @@ int srv_create(pk_server **out, pk_index *h, int traversal, int nslots, int32_t 
             cudaMallocHost((void **)&sl.h_ef, 4 * (size_t)max_batch) != cudaSuccess ||
             cudaMallocHost((void **)&sl.h_ids, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
             cudaMallocHost((void **)&sl.h_d, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
+            cudaMallocHost((void **)&sl.h_status, sizeof(int32_t)) != cudaSuccess ||
             cudaMalloc((void **)&sl.d_q, (size_t)max_batch * w) != cudaSuccess ||
             cudaMalloc((void **)&sl.d_k, 4 * (size_t)max_batch) != cudaSuccess ||
             cudaMalloc((void **)&sl.d_ef, 4 * (size_t)max_batch) != cudaSuccess ||
@@ -1793,6 +1893,18 @@ int pk_index_search_fast(pk_index *h, const void *queries, int64_t nq, int32_t k
     } catch (...) {
         return fail(PK_ERR_STATE, "pk_index_search_fast: unexpected exception");
     }
+}
+
+int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter_log2, int32_t warps_per_block) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    if (rows_per_batch < 0 || rows_per_batch > 256) return fail(PK_ERR_ARG, "rows_per_batch must be 0..256");
+    if (filter_log2 != 0 && (filter_log2 < 5 || filter_log2 > 15))
+        return fail(PK_ERR_ARG, "filter_log2 must be 0 or 5..15");
+    if (warps_per_block < 0 || warps_per_block > 8) return fail(PK_ERR_ARG, "warps_per_block must be 0..8");
+    h->fast_rb = rows_per_batch;
+    h->fast_hlog2 = filter_log2;
+    h->fast_wpb = warps_per_block;
+    return PK_OK;
 }
 
 int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from pickle_b200 import HNSWIndex, datasets
+from pickle_b200 import HNSWIndex, PickleError, datasets
 from tests.helpers import CASES, INTEGER_CASES, case_data, ref_graph
 
 pytestmark = pytest.mark.gpu
@@ -85,3 +85,82 @@ def test_fast_after_insert_covers_new_rows(gpu):
     fi, _ = idx.search_fast(queries, 10, 64)
     assert datasets.recall_at_k(fi, gt, 10) >= 0.9
     assert (fi >= 2000).any()
+
+
+def _valid_rows(fi, fd):
+    for row_i, row_d in zip(fi, fd):
+        valid = row_i >= 0
+        assert (np.diff(row_d[valid]) >= 0).all()
+        assert len(set(row_i[valid].tolist())) == valid.sum()
+
+
+# (rows per fetch batch, log2 of the recently-seen-id table, warps per block):
+# 32 table slots forget almost every id, so nearly every revisit recomputes a
+# distance; the list must still hold no repeats
+SHAPES = [(1, 5, 1), (8, 5, 2), (33, 7, 3), (64, 10, 4), (256, 15, 8)]
+
+
+@pytest.mark.parametrize("expand", [1, 2, 4])
+@pytest.mark.parametrize("shape", SHAPES)
+def test_fast_launch_shapes_keep_results(shape, expand, gpu, ref_bin):
+    metric, base, queries, M, efc = case_data("f32unit_ip")
+    idx = HNSWIndex.load(ref_graph("f32unit_ip"))
+    idx.prepare_fast("f16")
+    gt, _ = datasets.exact_knn(base, queries, 10, metric)
+    one, _ = idx.search_fast(queries, 10, 64)
+    di, dd = idx.search_fast(queries, 10, 64, expand=expand)
+    idx.set_fast_params(*shape)
+    fi, fd = idx.search_fast(queries, 10, 64, expand=expand)
+    _valid_rows(fi, fd)
+    # the list after each step is the best ef of what was listed and what
+    # was met, whatever the batch order, and a forgotten id is turned away or
+    # dropped as a repeat: the shape changes the work done, not the result
+    np.testing.assert_array_equal(fi, di)
+    np.testing.assert_array_equal(fd, dd)
+    r_one = datasets.recall_at_k(one, gt, 10)
+    r_exp = datasets.recall_at_k(fi, gt, 10)
+    assert r_exp >= r_one - 0.01, (r_exp, r_one)
+
+
+@pytest.mark.parametrize("ef", [1, 10, 33, 64, 65, 257, 512])
+def test_fast_list_sizes(ef, gpu, ref_bin):
+    """Every list width (1..16 slots per lane), k up to ef."""
+    metric, base, queries, M, efc = case_data("f32unit_ip")
+    idx = HNSWIndex.load(ref_graph("f32unit_ip"))
+    idx.prepare_fast("f16")
+    k = min(ef, 10)
+    fi, fd = idx.search_fast(queries, k, ef)
+    _valid_rows(fi, fd)
+    ei, _ = idx.search(queries, k, ef)
+    gt, _ = datasets.exact_knn(base, queries, k, metric)
+    assert datasets.recall_at_k(fi, gt, k) >= datasets.recall_at_k(ei, gt, k) - 0.02
+
+
+def test_fast_rejects_oversized_ef_and_shapes(gpu, ref_bin):
+    idx = HNSWIndex.load(ref_graph("f32unit_ip"))
+    idx.prepare_fast("f16")
+    _, _, queries, _, _ = case_data("f32unit_ip")
+    with pytest.raises(PickleError):
+        idx.search_fast(queries[:4], 10, 513)
+    for bad in [(-1, 0, 0), (257, 0, 0), (0, 4, 0), (0, 16, 0), (0, 0, 9)]:
+        with pytest.raises(PickleError):
+            idx.set_fast_params(*bad)
+
+
+def test_fast_rows_added_beyond_the_scale(gpu):
+    """FP16 rows added later at 100x the built magnitude rebuild the copy
+    with a new scale instead of overflowing half precision."""
+    base, queries = datasets.gmm_unit(3000, 100, 32, ncomp=16, seed=6)
+    idx = HNSWIndex(32, np.float32, "l2", M=8, ef_construction=64)
+    idx.build(base[:2000])
+    idx.prepare_fast("f16")
+    big = base[2000:] * 100.0
+    idx.add(big, np.arange(2000, 3000, dtype=np.int32))
+    allv = np.concatenate([base[:2000], big])
+    q = np.concatenate([queries[:50], queries[50:] * 100.0])
+    gt, _ = datasets.exact_knn(allv, q, 10, "l2")
+    fi, fd = idx.search_fast(q, 10, 64)
+    _valid_rows(fi, fd)
+    assert np.isfinite(fd).all()
+    ei, _ = idx.search(q, 10, 64)
+    assert datasets.recall_at_k(fi, gt, 10) >= datasets.recall_at_k(ei, gt, 10) - 0.02
