@@ -166,10 +166,10 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_query():
-    """DRAM bytes per query of the search kernel from the committed ncu summary."""
+def ncu_traffic_per_query(kernel):
+    """DRAM bytes per query of a kernel from its committed ncu summary."""
     try:
-        with open(os.path.join(ROOT, "profiles", "search_exact_1Mx96_traffic.json")) as f:
+        with open(os.path.join(ROOT, "profiles", f"{kernel}_1Mx96_traffic.json")) as f:
             return json.load(f)
     except (OSError, ValueError):
         return None
@@ -226,7 +226,6 @@ def run_ours(args):
     qh = torch.from_numpy(queries).pin_memory()
     ih = torch.empty((nq, k), dtype=torch.int32).pin_memory()
     dh = torch.empty((nq, k), dtype=torch.float32).pin_memory()
-    row_bytes = args.dim * 4
 
     def call(path, ef, counters=None):
         if path == "exact":
@@ -257,21 +256,30 @@ def run_ours(args):
                 break
         if ef is None:
             ef, recall = EF_SWEEP[-1], sweep[EF_SWEEP[-1]]
+        shape = None
+        if path != "exact":
+            # the launch shape for this batch (results do not depend on it)
+            shape, _ = idx.tune_fast(q_dev, k, ef, args.expand, stream)
         cnt = torch.zeros((nq, 6), dtype=torch.int32, device=dev)
         call(path, ef, counters=cnt)
         torch.cuda.synchronize()
         c = cnt.double().sum(0).cpu().numpy() / nq
         hops_u, dist_u, hops0, dist0 = c[0], c[1], c[3], c[4]
-        trav_bytes = {"exact": 4, "f16": 2, "fp8": 1}[path] * args.dim
-        rerank = 0 if path == "exact" else min(ef, dist0 + 1) * row_bytes
-        bpq = (dist_u + dist0) * trav_bytes + hops0 * 2 * args.M * 4 + hops_u * args.M * 4 + rerank
+        # algorithmic bytes per query of the dominant kernel: the rows whose
+        # distances it computes (traversal rows: f16 padded to 32 bytes,
+        # fp8 to 16) and the adjacency lists it reads
+        trav_bytes = {"exact": args.dim * 4, "f16": (args.dim * 2 + 31) // 32 * 32,
+                      "fp8": (args.dim + 15) // 16 * 16}[path]
+        bpq = (dist_u + dist0) * trav_bytes + hops0 * 2 * args.M * 4 + hops_u * args.M * 4
         for _ in range(args.warmup):
             call(path, ef)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        times = []
+        times, kernel_ms = [], []
+        if path != "exact":
+            idx.set_fast_timing(True)
         with ClockSampler(local) as clk:
             for _ in range(args.steps):
                 flush.fill_(1)
@@ -282,7 +290,12 @@ def run_ours(args):
                 b.record(stream)
                 b.synchronize()
                 times.append(a.elapsed_time(b))
+                # the dominant kernel alone: the walk (events the library
+                # records around it on this stream), or the exact search
+                kernel_ms.append(idx.fast_timing()[0] if path != "exact" else times[-1])
         torch.cuda.synchronize()
+        if path != "exact":
+            idx.set_fast_timing(False)
         total_ms = float(sum(times))
         if world > 1:
             t = torch.tensor([total_ms], device=dev)
@@ -304,7 +317,8 @@ def run_ours(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
         ms = total_ms / args.steps
-        return {"path": path, "ef": ef, "recall": recall, "sweep": sweep, "ms_per_step": ms,
+        return {"path": path, "ef": ef, "recall": recall, "sweep": sweep, "ms_per_step": ms, "shape": shape,
+                "kernel_ms": float(np.mean(kernel_ms)),
                 "qps": world * nq * args.steps / (total_ms / 1e3), "e2e_qps": world * nq * args.steps / e2e_s,
                 "bytes_per_query": bpq, "dist_evals": dist_u + dist0, "hops0": hops0, "hops_u": hops_u,
                 "clocks": clk.summary()}
@@ -317,11 +331,12 @@ def run_ours(args):
     ok = [r for r in results.values() if r["recall"] >= RECALL_TARGET] or list(results.values())
     best = max(ok, key=lambda r: r["qps"])
     peak, peak_kind = measured_peaks()
-    achieved = best["bytes_per_query"] * nq / (best["ms_per_step"] / 1e3) / 1e9
-    tr = ncu_traffic_per_query()
+    kernel = "search_exact_kernel" if best["path"] == "exact" else "walk_kernel"
+    achieved = best["bytes_per_query"] * nq / (best["kernel_ms"] / 1e3) / 1e9
+    tr = ncu_traffic_per_query(kernel)
     traffic = None
     if tr and tr.get("workload") == "1Mx96" and tr.get("path") == best["path"] and "dram_bytes_per_query" in tr:
-        traffic = tr["dram_bytes_per_query"] * nq
+        traffic = round(tr["dram_bytes_per_query"] * nq)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -352,16 +367,18 @@ def run_ours(args):
                        "recall_at_10": round(best["recall"], 4),
                        "paths": {p: {"ef": r["ef"], "recall_at_10": round(r["recall"], 4), "qps": round(r["qps"], 1),
                                      "e2e_qps": round(r["e2e_qps"], 1), "ms_per_step": round(r["ms_per_step"], 4),
+                                     "kernel_ms": round(r["kernel_ms"], 4), "launch_shape": r["shape"],
                                      "ef_sweep_recall": r["sweep"]} for p, r in results.items()},
                        "speedup_vs_plain_fp32": round(best["qps"] / plain["qps"], 3) if plain else None,
                        "l2": "flushed between steps (256 MiB write); index 640 MB > L2",
                        "build_s": round(build_s, 2), "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(best["e2e_qps"], 1), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * args.dim * 4, "d2h_bytes_per_step": nq * k * 8},
-            "gpu_launches": args.steps * (1 if best["path"] == "exact" else 2),
+            # exact: the search kernel; fast: query conversion, walk, re-rank
+            "gpu_launches": args.steps * (1 if best["path"] == "exact" else 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "search_exact_kernel" if best["path"] == "exact" else "search_fast_kernel",
+                         "kernel": kernel, "kernel_ms": round(best["kernel_ms"], 4),
                          "bytes_per_query": round(best["bytes_per_query"], 1),
                          "per_query": {"dist_evals": round(best["dist_evals"], 1), "hops_l0": round(best["hops0"], 1),
                                        "hops_upper": round(best["hops_u"], 1)}},

@@ -152,6 +152,25 @@ int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int3
  * recomputed distances); the speed does.  No counterpart in the reference. */
 int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter_log2, int32_t warps_per_block);
 
+/* Measurement: with timing enabled, each pk_index_search_fast /
+ * pk_index_search_fast_host call on the handle records CUDA events on its
+ * stream around the walk kernel and the re-rank kernel;
+ * pk_index_fast_timing waits for the last call's events and returns the two
+ * device durations in milliseconds.  Off by default (serving slots never
+ * record).  No counterpart in the reference. */
+int pk_index_set_fast_timing(pk_index *h, int enable);
+int pk_index_fast_timing(pk_index *h, float *walk_ms, float *rerank_ms);
+
+/* Autotuner: runs pk_index_search_fast on this batch (queries in device
+ * memory, uniform k and ef, `expand` as given) for a grid of launch shapes,
+ * times each with CUDA events on `stream`, and keeps the fastest as the
+ * handle's shape (as pk_index_set_fast_params would).  out_shape (3 ints,
+ * may be null) receives rows_per_batch, filter_log2, warps_per_block; out_ms
+ * (may be null) the batch time.  Synchronous; results of later searches are
+ * the same as with any other shape.  No counterpart in the reference. */
+int pk_index_tune_fast(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t expand,
+                       int32_t *out_shape, float *out_ms, void *stream);
+
 /* Serving: continuous batching over pk_index_search_fast.  No counterpart
  * in the reference (its batch AnnSearch is a blocking OpenMP loop,
  * include/hnsw.hpp:528-541).  A worker thread owns `slots` execution slots,

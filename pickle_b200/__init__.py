@@ -70,6 +70,9 @@ def lib() -> ctypes.CDLL:
         L.pk_index_search_fast.argtypes = [P, VP, I64, I32, I32, VP, VP, I32, VP, VP, VP, I32, VP]
         L.pk_index_search_fast_host.argtypes = [P, VP, I64, I32, I32, VP, VP, I32]
         L.pk_index_set_fast_params.argtypes = [P, I32, I32, I32]
+        L.pk_index_set_fast_timing.argtypes = [P, ctypes.c_int]
+        L.pk_index_fast_timing.argtypes = [P, VP, VP]
+        L.pk_index_tune_fast.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
         L.pk_index_search_noalloc.argtypes = [P, VP, I64, I32, I32, VP, VP, VP]
         L.pk_server_create.argtypes = [PP, P, ctypes.c_int, ctypes.c_int, I32, I32, I32, I32]
         L.pk_server_submit.argtypes = [P, VP, I32, I32, I32, ctypes.POINTER(ctypes.c_int64)]
@@ -192,6 +195,27 @@ class HNSWIndex:
         """Launch shape of the fast walk (0 = default): rows fetched per round trip, log2 of the
         recently-seen-id table's slots, warps per block.  Results do not depend on the shape."""
         _check(lib().pk_index_set_fast_params(self._h, rows_per_batch, filter_log2, warps_per_block))
+
+    def set_fast_timing(self, enable: bool) -> None:
+        """Record CUDA events around the walk and re-rank kernels of each fast search."""
+        _check(lib().pk_index_set_fast_timing(self._h, int(bool(enable))))
+
+    def fast_timing(self):
+        """(walk_ms, rerank_ms) of the last timed fast search (waits for it)."""
+        w = np.zeros(1, np.float32)
+        r = np.zeros(1, np.float32)
+        _check(lib().pk_index_fast_timing(self._h, _ptr(w), _ptr(r)))
+        return float(w[0]), float(r[0])
+
+    def tune_fast(self, queries, k: int, ef: int, expand: int = 1, stream=None):
+        """Time a grid of walk launch shapes on this batch (a torch CUDA tensor), keep the fastest;
+        returns ((rows_per_batch, filter_log2, warps_per_block), batch milliseconds)."""
+        shape = np.zeros(3, np.int32)
+        ms = np.zeros(1, np.float32)
+        s = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _check(lib().pk_index_tune_fast(self._h, _dev_ptr(queries), queries.shape[0], k, ef, expand, _ptr(shape),
+                                        _ptr(ms), s))
+        return tuple(int(x) for x in shape), float(ms[0])
 
     def search_fast_device(self, queries, k: int, ef: int, out_ids, out_dists, k_per_query=None, ef_per_query=None,
                            counters=None, expand: int = 1, stream=None) -> None:

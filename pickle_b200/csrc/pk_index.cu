@@ -118,6 +118,9 @@ struct FastCtx {
     int64_t fq_n = 0, tq_n = 0;
     float *d_qn = nullptr;
     int64_t qn_n = 0;
+    // optional timing of the last launch: before the walk, after it, after
+    // the re-rank (created on first use)
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
 };
 
 }  // namespace
@@ -169,6 +172,7 @@ struct pk_index {
     // walk launch shape (0 = the default): rows per fetch batch, log2 of the
     // visited-filter slots, warps per block
     int fast_rb = 0, fast_hlog2 = 0, fast_wpb = 0;
+    bool fast_timing = false;      // record events around the walk and the re-rank
 
     size_t dev_bytes = 0;
 
@@ -874,7 +878,14 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     a.trav_row_bytes = h->trav_row_bytes;
     a.trav_rows = h->trav_rows;
     a.rownorm = h->d_rownorm;
+    const bool timed = h->fast_timing && &c == &h->fctx;
+    if (timed) {
+        for (cudaEvent_t &e : c.ev)
+            if (!e) PK_CUDA(cudaEventCreate(&e));
+        PK_CUDA(cudaEventRecord(c.ev[0], s));
+    }
     PK_CUDA(pk::launch_walk(h->dg, h->trav, tc, slots, a, (int)grid, ws.wpb, ws.smem, s));
+    if (timed) PK_CUDA(cudaEventRecord(c.ev[1], s));
 
     int rwpb = 4;
     size_t rsmem = (size_t)rwpb * pk::rerank_layout(cs, h->row_bytes).total;
@@ -901,6 +912,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     r.queries = qx;
     r.row_bytes = h->row_bytes;
     PK_CUDA(pk::launch_rerank(h->dg, h->dtype, h->lc, r, (int)rgrid, rwpb, rsmem, s));
+    if (timed) PK_CUDA(cudaEventRecord(c.ev[2], s));
     return PK_OK;
 }
 
@@ -955,6 +967,8 @@ int init_handle(pk_index *h, int metric, int dtype, int64_t dim, int64_t M, int6
 }
 
 void free_fast_ctx(pk_index *h, FastCtx &c) {
+    for (cudaEvent_t &e : c.ev)
+        if (e) cudaEventDestroy(e);
     dfree(h, c.d_work, 4 * (size_t)c.work_n);
     dfree(h, c.d_cand, 4 * (size_t)c.cand_n);
     dfree(h, c.d_fq, (size_t)c.fq_n);
@@ -1317,6 +1331,86 @@ static int pk_index_prepare_fast_impl(pk_index *h, int traversal) {
     if (traversal != PK_TRAVERSAL_F16 && traversal != PK_TRAVERSAL_FP8)
         return fail(PK_ERR_ARG, "traversal must be PK_TRAVERSAL_F16 or PK_TRAVERSAL_FP8");
     return build_traversal(h, traversal == PK_TRAVERSAL_F16 ? pk::kTravF16 : pk::kTravE4M3);
+}
+
+// Times the walk + re-rank of this batch for a grid of launch shapes (rows
+// per fetch batch, visited-filter size, warps per block) and keeps the
+// fastest.  The result lists are the same for every shape; only the work
+// and its overlap change, so the choice is by time alone.
+static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                                   int32_t expand, int32_t *out_shape, float *out_ms, void *stream) {
+    if (!h || !queries || nq < 1 || k < 1 || ef < k) return fail(PK_ERR_ARG, "bad arguments");
+    if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
+    if (h->n0() == 0) return fail(PK_ERR_STATE, "the index is empty");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    PK_TRY(ensure_buf(h, &h->d_fids, h->fids_n, nq * k));
+    PK_TRY(ensure_buf(h, &h->d_fdists, h->fdists_n, nq * k));
+    const int keep_rb = h->fast_rb, keep_h = h->fast_hlog2, keep_w = h->fast_wpb;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PK_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(PK_ERR_CUDA, "cudaEventCreate failed");
+    }
+    float best = -1.f;
+    int brb = 0, bh = 0, bw = 0;
+    int rc = PK_OK;
+    const int rbs[] = {16, 24, 32, 48, 64};
+    const int hls[] = {8, 9, 10, 11};
+    const int wps[] = {2, 4};
+    for (int rb : rbs) {
+        for (int hl : hls) {
+            for (int wp : wps) {
+                h->fast_rb = rb;
+                h->fast_hlog2 = hl;
+                h->fast_wpb = wp;
+                WalkShape ws;
+                if (walk_shape(h, ws) != PK_OK || ws.wpb != wp) continue;  // does not fit
+                float ms = 0.f;
+                for (int rep = 0; rep < 3 && rc == PK_OK; rep++) {
+                    if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(PK_ERR_CUDA, "cudaEventRecord failed");
+                    if (rc == PK_OK)
+                        rc = run_search_fast(h, h->fctx, queries, false, nq, k, ef, nullptr, nullptr, k, h->d_fids,
+                                             h->d_fdists, nullptr, expand, s);
+                    if (rc == PK_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+                        rc = fail(PK_ERR_CUDA, "tuning launch failed");
+                    float t = 0.f;
+                    if (rc == PK_OK && cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+                        rc = fail(PK_ERR_CUDA, "cudaEventElapsedTime failed");
+                    if (rep > 0) ms += t;  // the first run warms caches
+                }
+                if (rc != PK_OK) break;
+                ms /= 2.f;
+                if (best < 0.f || ms < best) {
+                    best = ms;
+                    brb = rb;
+                    bh = hl;
+                    bw = wp;
+                }
+            }
+            if (rc != PK_OK) break;
+        }
+        if (rc != PK_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == PK_OK) rc = fast_status(h, h->fctx, s);
+    if (rc != PK_OK || best < 0.f) {
+        h->fast_rb = keep_rb;
+        h->fast_hlog2 = keep_h;
+        h->fast_wpb = keep_w;
+        return rc != PK_OK ? rc : fail(PK_ERR_ARG, "no launch shape fits this index");
+    }
+    h->fast_rb = brb;
+    h->fast_hlog2 = bh;
+    h->fast_wpb = bw;
+    if (out_shape) {
+        out_shape[0] = brb;
+        out_shape[1] = bh;
+        out_shape[2] = bw;
+    }
+    if (out_ms) *out_ms = best;
+    return PK_OK;
 }
 
 static int pk_index_search_fast_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
@@ -1882,6 +1976,17 @@ int pk_index_prepare_fast(pk_index *h, int traversal) {
     }
 }
 
+int pk_index_tune_fast(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t expand,
+                       int32_t *out_shape, float *out_ms, void *stream) {
+    try {
+        return pk_index_tune_fast_impl(h, queries, nq, k, ef, expand, out_shape, out_ms, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_tune_fast: unexpected exception");
+    }
+}
+
 int pk_index_search_fast(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
                          const int32_t *k_per_query, const int32_t *ef_per_query, int32_t out_stride, int32_t *out_ids,
                          float *out_dists, int32_t *counters, int32_t expand, void *stream) {
@@ -1904,6 +2009,22 @@ int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter
     h->fast_rb = rows_per_batch;
     h->fast_hlog2 = filter_log2;
     h->fast_wpb = warps_per_block;
+    return PK_OK;
+}
+
+int pk_index_set_fast_timing(pk_index *h, int enable) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    h->fast_timing = enable != 0;
+    return PK_OK;
+}
+
+int pk_index_fast_timing(pk_index *h, float *walk_ms, float *rerank_ms) {
+    if (!h || !walk_ms || !rerank_ms) return fail(PK_ERR_ARG, "bad arguments");
+    const FastCtx &c = h->fctx;
+    if (!h->fast_timing || !c.ev[2]) return fail(PK_ERR_STATE, "no timed fast search has run");
+    PK_CUDA(cudaEventSynchronize(c.ev[2]));
+    PK_CUDA(cudaEventElapsedTime(walk_ms, c.ev[0], c.ev[1]));
+    PK_CUDA(cudaEventElapsedTime(rerank_ms, c.ev[1], c.ev[2]));
     return PK_OK;
 }
 

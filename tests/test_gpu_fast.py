@@ -164,3 +164,57 @@ def test_fast_rows_added_beyond_the_scale(gpu):
     assert np.isfinite(fd).all()
     ei, _ = idx.search(q, 10, 64)
     assert datasets.recall_at_k(fi, gt, 10) >= datasets.recall_at_k(ei, gt, 10) - 0.02
+
+
+def test_tuner_keeps_results_and_picks_a_valid_shape(gpu, ref_bin):
+    import torch
+    metric, base, queries, M, efc = case_data("f32unit_ip")
+    idx = HNSWIndex.load(ref_graph("f32unit_ip"))
+    idx.prepare_fast("f16")
+    di, dd = idx.search_fast(queries, 10, 48)
+    shape, ms = idx.tune_fast(torch.from_numpy(queries).cuda(), 10, 48)
+    assert shape[0] in (16, 24, 32, 48, 64) and shape[1] in (8, 9, 10, 11) and shape[2] in (2, 4)
+    assert ms > 0
+    fi, fd = idx.search_fast(queries, 10, 48)
+    np.testing.assert_array_equal(fi, di)
+    np.testing.assert_array_equal(fd, dd)
+
+
+def test_fast_search_replays_from_a_cuda_graph(gpu, ref_bin):
+    """One captured launch sequence (traversal prep, walk, re-rank) answers
+    new queries copied into the same input buffer."""
+    import torch
+    metric, base, queries, M, efc = case_data("f32unit_ip")
+    idx = HNSWIndex.load(ref_graph("f32unit_ip"))
+    idx.prepare_fast("f16")
+    nq = len(queries) // 2
+    qa, qb = queries[:nq], queries[nq:2 * nq]
+    q = torch.from_numpy(qa).cuda()
+    ids = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+    ds = torch.empty((nq, 10), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        idx.search_fast_device(q, 10, 48, ids, ds, stream=stream)  # grows the buffers
+    stream.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        idx.search_fast_device(q, 10, 48, ids, ds, stream=torch.cuda.current_stream())
+    for part in (qa, qb, qa):
+        q.copy_(torch.from_numpy(part))
+        g.replay()
+        torch.cuda.synchronize()
+        wi, wd = idx.search_fast(part, 10, 48)
+        np.testing.assert_array_equal(ids.cpu().numpy(), wi)
+        np.testing.assert_array_equal(ds.cpu().numpy(), wd)
+
+
+def test_fast_timing_events(gpu, ref_bin):
+    metric, base, queries, M, efc = case_data("f32unit_ip")
+    idx = HNSWIndex.load(ref_graph("f32unit_ip"))
+    idx.prepare_fast("f16")
+    with pytest.raises(PickleError):
+        idx.fast_timing()
+    idx.set_fast_timing(True)
+    idx.search_fast(queries, 10, 48)
+    walk_ms, rerank_ms = idx.fast_timing()
+    assert walk_ms > 0 and rerank_ms > 0
