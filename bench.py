@@ -43,7 +43,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC_NAME = "QPS at recall@10>=0.95 (1M x 96 f32, IP, M=32, efC=400, k=10)"
-EF_SWEEP = [16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512]
+EF_SWEEP = [16, 24, 32, 36, 40, 44, 48, 56, 64, 80, 96, 112, 128, 160, 192, 256, 320, 384, 512]
 RECALL_TARGET = 0.95
 
 
@@ -65,6 +65,7 @@ def parse():
     p.add_argument("--verbose", action="store_true")
     p.add_argument("--paths", default="exact,f16,fp8", help="search paths to measure (exact, f16, fp8)")
     p.add_argument("--expand", type=int, default=1, help="entries expanded per step on the fast paths")
+    p.add_argument("--fast-shape", default="", help="rows,filter_log2,warps for the fast walk instead of tuning")
     return p.parse_args()
 
 
@@ -259,18 +260,36 @@ def run_ours(args):
         shape = None
         if path != "exact":
             # the launch shape for this batch (results do not depend on it)
-            shape, _ = idx.tune_fast(q_dev, k, ef, args.expand, stream)
-        cnt = torch.zeros((nq, 6), dtype=torch.int32, device=dev)
-        call(path, ef, counters=cnt)
-        torch.cuda.synchronize()
-        c = cnt.double().sum(0).cpu().numpy() / nq
+            if args.fast_shape:
+                shape = tuple(int(x) for x in args.fast_shape.split(","))
+                idx.set_fast_params(*shape)
+            else:
+                shape, _ = idx.tune_fast(q_dev, k, ef, args.expand, stream)
+
+        def per_query_counts():
+            cnt = torch.zeros((nq, 6), dtype=torch.int32, device=dev)
+            call(path, ef, counters=cnt)
+            torch.cuda.synchronize()
+            return cnt.double().sum(0).cpu().numpy() / nq
+
+        c = per_query_counts()
+        fetched = c[1] + c[4]
+        if path != "exact":
+            # the tuned walk forgets ids in its small recently-seen table and
+            # fetches some rows again; a 32768-slot table forgets almost
+            # none, so its count is the (near) unique rows the walk needs
+            idx.set_fast_params(shape[0], 15, 1)
+            c = per_query_counts()
+            idx.set_fast_params(*shape)
         hops_u, dist_u, hops0, dist0 = c[0], c[1], c[3], c[4]
         # algorithmic bytes per query of the dominant kernel: the rows whose
-        # distances it computes (traversal rows: f16 padded to 32 bytes,
-        # fp8 to 16) and the adjacency lists it reads
+        # distances it needs (traversal rows: f16 padded to 32 bytes, fp8 to
+        # 16) and the adjacency lists it reads
         trav_bytes = {"exact": args.dim * 4, "f16": (args.dim * 2 + 31) // 32 * 32,
                       "fp8": (args.dim + 15) // 16 * 16}[path]
-        bpq = (dist_u + dist0) * trav_bytes + hops0 * 2 * args.M * 4 + hops_u * args.M * 4
+        adj_bytes = hops0 * 2 * args.M * 4 + hops_u * args.M * 4
+        bpq = (dist_u + dist0) * trav_bytes + adj_bytes
+        fetched_bpq = fetched * trav_bytes + adj_bytes
         for _ in range(args.warmup):
             call(path, ef)
         torch.cuda.synchronize()
@@ -318,6 +337,7 @@ def run_ours(args):
             e2e_s = float(t.item())
         ms = total_ms / args.steps
         return {"path": path, "ef": ef, "recall": recall, "sweep": sweep, "ms_per_step": ms, "shape": shape,
+                "fetched_bytes_per_query": fetched_bpq, "rows_fetched": fetched,
                 "kernel_ms": float(np.mean(kernel_ms)),
                 "qps": world * nq * args.steps / (total_ms / 1e3), "e2e_qps": world * nq * args.steps / e2e_s,
                 "bytes_per_query": bpq, "dist_evals": dist_u + dist0, "hops0": hops0, "hops_u": hops_u,
@@ -380,8 +400,10 @@ def run_ours(args):
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                          "kernel": kernel, "kernel_ms": round(best["kernel_ms"], 4),
                          "bytes_per_query": round(best["bytes_per_query"], 1),
+                         "fetched_bytes_per_query": round(best["fetched_bytes_per_query"], 1),
                          "per_query": {"dist_evals": round(best["dist_evals"], 1), "hops_l0": round(best["hops0"], 1),
-                                       "hops_upper": round(best["hops_u"], 1)}},
+                                       "hops_upper": round(best["hops_u"], 1),
+                                       "rows_fetched": round(best["rows_fetched"], 1)}},
             "cpu_baseline": cpu,
             "clocks": best["clocks"],
         }
