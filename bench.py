@@ -355,7 +355,8 @@ def run_ours(args):
     achieved = best["bytes_per_query"] * nq / (best["kernel_ms"] / 1e3) / 1e9
     tr = ncu_traffic_per_query(kernel)
     traffic = None
-    if tr and tr.get("workload") == "1Mx96" and tr.get("path") == best["path"] and "dram_bytes_per_query" in tr:
+    if (tr and tr.get("workload") == "1Mx96" and tr.get("path") == best["path"] and tr.get("ef") == best["ef"]
+            and "dram_bytes_per_query" in tr):
         traffic = round(tr["dram_bytes_per_query"] * nq)
 
     cpu = None

@@ -1,0 +1,173 @@
+"""Search benchmark over the configurations beyond the headline one.
+
+    python -m pickle_b200.config_bench --config c1|c3u8|c3i8|c4 [--paths exact,f16,fp8] [--n N] [--nq NQ]
+                                       [--cpu-sample Q]
+
+Each configuration is a seeded synthetic stand-in with the shape, type,
+metric and graph parameters of one of the reference's benchmark datasets
+(the public files are not available offline):
+
+  c1    100k x 128 integer-valued float32 (64-component mixture, centres in
+        [0, 255], sigma 20, rounded and clipped), L2, M=16, efC=200,
+        10k queries, k=10, ef in {16, 32, 64, 128, 256}
+  c3u8  1M x 128 uint8 (sigma 12), L2 in int32, M=16, efC=200, 10k queries
+  c3i8  the same in int8
+  c4    10M x 128 float16 (1024-component mixture, sigma 0.5), L2, M=32,
+        efC=200, 100k queries each with its own k in {1, 10, 100} and ef
+        uniform in [max(k, 16), 512] (one mixed batch)
+
+The index is built on the GPU.  Per path (exact = the reference's search;
+f16 / fp8 = low-precision walk plus exact re-rank, launch shape tuned on the
+batch) and ef, one JSON line: queries/s from CUDA events around whole
+batches (L2 flushed before each batch, median of the timed batches),
+recall@k against exact float64 ground truth, per-query distance evaluations.
+With --cpu-sample, the reference's own search (the oracle harness built from
+the reference sources, when present) is timed on the saved graph on all host
+threads for a sample of the queries at one ef.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+
+CONFIGS = {
+    "c1": dict(n=100_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256]),
+    "c3u8": dict(n=1_000_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256]),
+    "c3i8": dict(n=1_000_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256]),
+    "c4": dict(n=10_000_000, nq=100_000, dim=128, metric="l2", M=32, efc=200, efs=None),
+}
+
+
+def make(cfg_name, n, nq, seed):
+    from pickle_b200 import datasets
+    c = CONFIGS[cfg_name]
+    if cfg_name == "c1":
+        return datasets.gmm_int_f32(n, nq, c["dim"], ncomp=64, sigma=20.0, seed=seed)
+    if cfg_name in ("c3u8", "c3i8"):
+        return datasets.gmm_bytes(n, nq, c["dim"], ncomp=256, sigma=12.0, signed=cfg_name == "c3i8", seed=seed)
+    return datasets.gmm_f16(n, nq, c["dim"], ncomp=1024, sigma=0.5, seed=seed)
+
+
+def recall_mixed(found, truth, ks):
+    hit = 0
+    for f, t, k in zip(found, truth, ks):
+        hit += len(set(int(x) for x in f[:k] if x >= 0) & set(int(x) for x in t[:k]))
+    return hit / float(np.sum(ks))
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--config", required=True, choices=sorted(CONFIGS))
+    p.add_argument("--paths", default="exact,f16,fp8")
+    p.add_argument("--n", type=int, default=0)
+    p.add_argument("--nq", type=int, default=0)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--cpu-sample", type=int, default=0, help="queries timed on the reference's CPU search")
+    a = p.parse_args(argv)
+
+    import torch
+
+    from pickle_b200 import HNSWIndex, datasets
+    from pickle_b200.groundtruth import gpu_knn
+    c = CONFIGS[a.config]
+    n, nq = a.n or c["n"], a.nq or c["nq"]
+    t0 = time.time()
+    base, queries = make(a.config, n, nq, a.seed)
+    gen_s = time.time() - t0
+    idx = HNSWIndex(c["dim"], base.dtype, c["metric"], M=c["M"], ef_construction=c["efc"])
+    idx.set_seed(a.seed)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    idx.build(base)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    info = idx.info()
+    dev = torch.device("cuda")
+    mixed = c["efs"] is None
+    kmax = 100 if mixed else 10
+    t0 = time.time()
+    gt = gpu_knn(base, queries, kmax, c["metric"], dev)
+    gt_s = time.time() - t0
+    head = {"config": a.config, "n": n, "nq": nq, "dim": c["dim"], "dtype": str(base.dtype), "metric": c["metric"],
+            "M": c["M"], "ef_construction": c["efc"], "gen_s": round(gen_s, 1), "build_s": round(build_s, 1),
+            "gt_s": round(gt_s, 1), "device_mb": info["device_bytes"] >> 20}
+    print(json.dumps(dict(head, event="built")), flush=True)
+
+    q = torch.from_numpy(queries).to(dev)
+    rng = np.random.default_rng(a.seed + 7)
+    if mixed:
+        ks = rng.choice([1, 10, 100], size=nq).astype(np.int32)
+        efs_q = np.array([rng.integers(max(int(k), 16), 513) for k in ks], np.int32)
+        k_dev, ef_dev = torch.from_numpy(ks).to(dev), torch.from_numpy(efs_q).to(dev)
+        runs = [("mixed", int(ks.max()), int(efs_q.max()))]
+    else:
+        ks = np.full(nq, 10, np.int32)
+        k_dev = ef_dev = None
+        runs = [(str(e), 10, e) for e in c["efs"]]
+    stride = int(ks.max())
+    ids = torch.empty((nq, stride), dtype=torch.int32, device=dev)
+    ds = torch.empty((nq, stride), dtype=torch.float32, device=dev)
+    cnt = torch.zeros((nq, 6), dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def call(path, k, ef, counters=None):
+        if path == "exact":
+            idx.search_device(q, k, ef, ids, ds, k_per_query=k_dev, ef_per_query=ef_dev, counters=counters)
+        else:
+            idx.search_fast_device(q, k, ef, ids, ds, k_per_query=k_dev, ef_per_query=ef_dev, counters=counters)
+
+    for path in a.paths.split(","):
+        if path != "exact":
+            idx.prepare_fast(path)
+        for label, k, ef in runs:
+            if path != "exact" and ef > 512:
+                continue
+            shape = None
+            if path != "exact":
+                shape, _ = idx.tune_fast(q, k, min(ef, 512))
+            call(path, k, ef)
+            torch.cuda.synchronize()
+            times = []
+            for step in range(a.steps + 1):
+                flush.fill_(1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                call(path, k, ef)
+                e1.record()
+                e1.synchronize()
+                if step:
+                    times.append(e0.elapsed_time(e1))
+            ms = float(np.median(times))
+            got = ids.cpu().numpy()
+            rec = recall_mixed(got, gt, ks)
+            cnt.zero_()
+            call(path, k, ef, counters=cnt)
+            torch.cuda.synchronize()
+            cc = cnt.double().mean(0).cpu().numpy()
+            print(json.dumps(dict(head, event="search", path=path, ef=label, k=("mixed {1,10,100}" if mixed else k),
+                                  qps=round(nq / ms * 1e3, 1), ms_per_batch=round(ms, 3), recall=round(rec, 4),
+                                  dist_per_query=round(float(cc[1] + cc[4]), 1),
+                                  hops_l0=round(float(cc[3]), 1), launch_shape=shape)), flush=True)
+
+    if a.cpu_sample:
+        import oracle
+        if oracle.ref_available():
+            ef = runs[len(runs) // 2][2] if not mixed else 64
+            with tempfile.TemporaryDirectory() as td:
+                gp = os.path.join(td, "g.pkg")
+                idx.save(gp)
+                sample = queries[:a.cpu_sample]
+                threads = os.cpu_count() or 1
+                _, _, ci = oracle.ref_search(gp, sample, 10, ef, threads=threads, repeat=3, want_results=False)
+            print(json.dumps(dict(head, event="cpu_reference", ef=ef, k=10, qps=round(ci["qps"], 1), cores=threads,
+                                  sample=len(sample))), flush=True)
+
+
+if __name__ == "__main__":
+    main()

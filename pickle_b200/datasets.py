@@ -34,14 +34,16 @@ def gmm_unit(n: int, nq: int, dim: int = 96, ncomp: int = 256, sigma: float = 0.
     else:
         w = 1.0 / np.arange(1, ncomp + 1) ** zipf_s
         lab = rng.choice(ncomp, size=n + nq, p=w / w.sum())
-    x = np.empty((n + nq, dim), np.float32)
+    # filled chunk by chunk in the target type (rounded through float32 as a
+    # whole-array conversion would be), so large float16 sets never hold a
+    # float32 copy
+    x = np.empty((n + nq, dim), dtype)
     step = 1 << 18
     for i in range(0, n + nq, step):
         j = min(n + nq, i + step)
         y = centres[lab[i:j]] + rng.normal(0, sigma / np.sqrt(dim), size=(j - i, dim))
         y /= np.linalg.norm(y, axis=1, keepdims=True)
-        x[i:j] = y
-    x = x.astype(dtype)
+        x[i:j] = y.astype(np.float32).astype(dtype)
     return x[:n], x[n:]
 
 
