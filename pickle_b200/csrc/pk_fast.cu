@@ -17,7 +17,8 @@
 //   * on layer 0 the result set is a sorted list of ef entries held in
 //     registers (lane l owns entries l*S .. l*S+S-1); each iteration expands
 //     the `expand` best unexpanded entries, filters their neighbours through
-//     a small direct-mapped table of recently seen ids in shared memory,
+//     a small table of recently seen ids in shared memory (2-way sets,
+//     least recently inserted out),
 //     fetches the new rows with one bulk copy (cp.async.bulk) per row onto a
 //     per-warp mbarrier, and inserts what beats the worst listed entry;
 //   * the walk ends when the first ef entries are all expanded, and their
@@ -405,7 +406,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
     const int enter_level = gp->enter_level;
     const int rb = a.rb;
     const int H = 1 << a.hlog2;
-    const int hshift = 32 - a.hlog2;
+    const int sshift = 33 - a.hlog2;  // 2^(hlog2 - 1) sets of two slots
     const int expand = max(1, min(a.expand, 4));
     const DevLayer L0 = gp->L[0];
     const int64_t lim0 = min(L0.lcap, a.trav_rows);
@@ -522,7 +523,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             if (lane == 0) {
                 list.d[0] = d0;
                 list.id[0] = (uint32_t)enter;
-                tab[((uint32_t)enter * 2654435769u) >> hshift] = enter;
+                reinterpret_cast<int2 *>(tab)[((uint32_t)enter * 2654435769u) >> sshift] = make_int2(enter, -1);
             }
             __syncwarp();
             list.at(wl, wsl, wd, wi, lane);
@@ -588,9 +589,11 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                     if (j < deg) v = (j < L0.cap && j0 == 0) ? pa0[p] : (j < L0.cap && j0 == 32) ? pa1[p] : L0.adj[base + j];
                     bool fresh = false;
                     if (v >= 0 && v < lim0) {
-                        int32_t *slot = tab + (((uint32_t)v * 2654435769u) >> hshift);
-                        if (*slot != v) {
-                            *slot = v;
+                        // 2-way set of the table: the most recent id first
+                        int2 *set = reinterpret_cast<int2 *>(tab) + (((uint32_t)v * 2654435769u) >> sshift);
+                        const int2 w = *set;
+                        if (w.x != v && w.y != v) {
+                            *set = make_int2(v, w.x);
                             fresh = true;
                         }
                     }

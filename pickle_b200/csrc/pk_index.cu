@@ -1355,43 +1355,49 @@ static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq,
     float best = -1.f;
     int brb = 0, bh = 0, bw = 0;
     int rc = PK_OK;
-    const int rbs[] = {16, 24, 32, 48, 64};
-    const int hls[] = {8, 9, 10, 11};
-    const int wps[] = {2, 4};
-    for (int rb : rbs) {
-        for (int hl : hls) {
-            for (int wp : wps) {
-                h->fast_rb = rb;
-                h->fast_hlog2 = hl;
-                h->fast_wpb = wp;
-                WalkShape ws;
-                if (walk_shape(h, ws) != PK_OK || ws.wpb != wp) continue;  // does not fit
-                float ms = 0.f;
-                for (int rep = 0; rep < 3 && rc == PK_OK; rep++) {
-                    if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(PK_ERR_CUDA, "cudaEventRecord failed");
-                    if (rc == PK_OK)
-                        rc = run_search_fast(h, h->fctx, queries, false, nq, k, ef, nullptr, nullptr, k, h->d_fids,
-                                             h->d_fdists, nullptr, expand, s);
-                    if (rc == PK_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
-                        rc = fail(PK_ERR_CUDA, "tuning launch failed");
-                    float t = 0.f;
-                    if (rc == PK_OK && cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
-                        rc = fail(PK_ERR_CUDA, "cudaEventElapsedTime failed");
-                    if (rep > 0) ms += t;  // the first run warms caches
-                }
-                if (rc != PK_OK) break;
-                ms /= 2.f;
-                if (best < 0.f || ms < best) {
-                    best = ms;
-                    brb = rb;
-                    bh = hl;
-                    bw = wp;
-                }
-            }
-            if (rc != PK_OK) break;
+    // times one shape (the first of three runs warms caches); false if it
+    // does not fit or a launch failed (rc set)
+    auto time_shape = [&](int rb, int hl, int wp) -> bool {
+        h->fast_rb = rb;
+        h->fast_hlog2 = hl;
+        h->fast_wpb = wp;
+        WalkShape ws;
+        if (walk_shape(h, ws) != PK_OK || ws.wpb != wp) return false;
+        float ms = 0.f;
+        for (int rep = 0; rep < 3 && rc == PK_OK; rep++) {
+            if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(PK_ERR_CUDA, "cudaEventRecord failed");
+            if (rc == PK_OK)
+                rc = run_search_fast(h, h->fctx, queries, false, nq, k, ef, nullptr, nullptr, k, h->d_fids,
+                                     h->d_fdists, nullptr, expand, s);
+            if (rc == PK_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+                rc = fail(PK_ERR_CUDA, "tuning launch failed");
+            float t = 0.f;
+            if (rc == PK_OK && cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+                rc = fail(PK_ERR_CUDA, "cudaEventElapsedTime failed");
+            if (rep > 0) ms += t;
         }
-        if (rc != PK_OK) break;
-    }
+        if (rc != PK_OK) return false;
+        ms /= 2.f;
+        if (best < 0.f || ms < best) {
+            best = ms;
+            brb = rb;
+            bh = hl;
+            bw = wp;
+        }
+        return true;
+    };
+    // stage 1: visited-table size and warps per block at 32 rows per batch
+    // (the table trades re-fetched rows against occupancy, more so as ef
+    // grows); stage 2: rows per batch at the best pair
+    const int hls[] = {8, 9, 10, 11, 12, 13};
+    const int wps[] = {1, 2, 4};
+    for (int hl : hls)
+        for (int wp : wps)
+            if (rc == PK_OK) time_shape(32, hl, wp);
+    const int h1 = bh, w1 = bw;
+    const int rbs[] = {16, 24, 48, 64};
+    for (int rb : rbs)
+        if (rc == PK_OK && best >= 0.f) time_shape(rb, h1, w1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc == PK_OK) rc = fast_status(h, h->fctx, s);

@@ -173,7 +173,7 @@ def test_tuner_keeps_results_and_picks_a_valid_shape(gpu, ref_bin):
     idx.prepare_fast("f16")
     di, dd = idx.search_fast(queries, 10, 48)
     shape, ms = idx.tune_fast(torch.from_numpy(queries).cuda(), 10, 48)
-    assert shape[0] in (16, 24, 32, 48, 64) and shape[1] in (8, 9, 10, 11) and shape[2] in (2, 4)
+    assert shape[0] in (16, 24, 32, 48, 64) and shape[1] in range(8, 14) and shape[2] in (1, 2, 4)
     assert ms > 0
     fi, fd = idx.search_fast(queries, 10, 48)
     np.testing.assert_array_equal(fi, di)
