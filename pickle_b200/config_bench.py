@@ -201,8 +201,9 @@ def main(argv=None):
             # returned distances against float64 for the returned ids (a sample)
             ns = min(nq, 2000)
             gd = ds.cpu().numpy()[:ns, :10]
-            gi = got[:ns, :10]
-            ok = gi >= 0
+            # a row holds results up to its own k only
+            ok = (got[:ns, :10] >= 0) & (np.arange(10)[None, :] < ks[:ns, None])
+            gi = np.where(ok, got[:ns, :10], 0)
             ex = exact_dist(base, queries[:ns], gi, c["metric"])
             rel = np.abs(gd - ex)[ok] / np.maximum(np.abs(ex[ok]), 1e-30)
             dist_err = {"max_rel": float(rel.max()), "median_rel": float(np.median(rel))}
