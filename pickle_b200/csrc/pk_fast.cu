@@ -412,12 +412,13 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
     const int64_t lim0 = min(L0.lcap, a.trav_rows);
     const float kInf = __int_as_float(0x7f800000);
 
+    const int64_t nlim = a.qcount ? (int64_t)*a.qcount : a.nq;
     for (;;) {
         int qi = 0;
         if (lane == 0) qi = atomicAdd(a.work, 1);
         qi = __shfl_sync(kFull, qi, 0);
-        if (qi >= a.nq) break;
-        const int64_t q = qi;
+        if (qi >= nlim) break;
+        const int64_t q = a.qlist ? a.qlist[qi] : qi;
         const int L = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, 32 * S));
 
         // the query in the traversal format: FP16 staged in shared memory,
@@ -606,7 +607,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             if (!failed && n > 0 && !flush0(n)) failed = true;
         }
         if (failed) {
-            if (lane == 0) atomicExch(a.work + 1, 1);
+            if (lane == 0) atomicExch(a.status, 1);
             return;
         }
 
@@ -711,6 +712,18 @@ __global__ void __launch_bounds__(128)
             od[i] = have ? sd[i] : FLT_MAX;
         }
         __syncwarp();
+    }
+}
+
+// Queries by list slots per lane: a walk launch per class then pays for the
+// list width its queries need, not the batch's widest.
+__global__ void bin_by_slots_kernel(const int32_t *ef_arr, int32_t ef_bound, int64_t nq, int32_t *counts,
+                                    int32_t *lists) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (int64_t)gridDim.x * blockDim.x) {
+        const int ef = max(1, min(ef_arr[q], ef_bound));
+        const int c = __ffs(list_slots(ef)) - 1;
+        const int pos = atomicAdd(counts + c, 1);
+        lists[(int64_t)c * nq + pos] = (int32_t)q;
     }
 }
 
@@ -900,6 +913,13 @@ cudaError_t launch_walk(const DevGraph *g, int trav, const TravCfgHost &tch, int
     TravCfg tc{tch.GT, tch.KT, tch.CT};
     void *args[] = {(void *)&g, (void *)&tc, (void *)&a};
     return cudaLaunchKernel(fn, dim3(grid), dim3(wpb * 32), args, smem, s);
+}
+
+cudaError_t launch_bin_by_slots(const int32_t *ef_arr, int32_t ef_bound, int64_t nq, int32_t *counts,
+                                int32_t *lists, cudaStream_t s) {
+    const int grid = (int)std::min<int64_t>((nq + 255) / 256, 1024);
+    bin_by_slots_kernel<<<std::max(grid, 1), 256, 0, s>>>(ef_arr, ef_bound, nq, counts, lists);
+    return cudaGetLastError();
 }
 
 int rerank_blocks_per_sm(int dtype, const LaneCfg &lc, int wpb, size_t smem) {

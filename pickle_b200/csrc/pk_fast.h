@@ -22,7 +22,10 @@ struct WalkArgs {
     int32_t expand;             // list entries expanded per iteration (1..4)
     const int32_t *ef_arr;
     int32_t *counters;          // nq * 6 or null
-    int32_t *work;              // [0] query counter, [1] status: 1 = a row fetch timed out
+    int32_t *work;              // this launch's query counter
+    int32_t *status;            // set to 1 when a row fetch timed out
+    const int32_t *qlist;       // the queries this launch takes (null: 0 .. nq-1)
+    const int32_t *qcount;      // their number, on the device (null: nq)
     int32_t *cand;              // nq * cand_stride: each query's final list (ids, -1 = empty)
     int32_t cand_stride;        // 32 * list slots per lane
     int32_t rb;                 // rows per fetch batch
@@ -97,7 +100,19 @@ __host__ __device__ inline RerankLayout rerank_layout(int cand_stride, int64_t r
     return r;
 }
 
+// List slots per lane (1, 2, 4, 8, 16) for an ef: the register list holds 32 per slot.
+__host__ __device__ inline int list_slots(int ef) {
+    int s = 1;
+    while (32 * s < ef && s < kFastMaxEf / 32) s *= 2;
+    return s;
+}
+constexpr int kSlotClasses = 5;  // slots 1, 2, 4, 8, 16
+
 int walk_blocks_per_sm(int trav, const TravCfgHost &tc, int slots, int wpb, size_t smem);
+// Sorts the queries by list slots: lists[c * nq + i] = the i-th query with
+// 2^c slots, counts[c] = how many (counts zeroed by the caller).
+cudaError_t launch_bin_by_slots(const int32_t *ef_arr, int32_t ef_bound, int64_t nq, int32_t *counts,
+                                int32_t *lists, cudaStream_t s);
 cudaError_t launch_walk(const DevGraph *g, int trav, const TravCfgHost &tc, int slots, const WalkArgs &a, int grid,
                         int wpb, size_t smem, cudaStream_t s);
 int rerank_blocks_per_sm(int dtype, const LaneCfg &lc, int wpb, size_t smem);

@@ -109,9 +109,18 @@ struct SearchScratch {
 
 // Per-launch working set of the fast search: scratch and query staging.  The
 // handle owns one; each serving slot owns its own, so slots can overlap.
+// Layout of FastCtx::d_work: the walk's status, the query count of each list
+// width class, the work counter of each class's launch.
+constexpr int kWorkStatus = 0;
+constexpr int kWorkCounts = 2;
+constexpr int kWorkCounters = kWorkCounts + pk::kSlotClasses;
+constexpr int kWorkInts = kWorkCounters + pk::kSlotClasses;
+
 struct FastCtx {
-    int32_t *d_work = nullptr;     // [0] query counter of the walk, [1] its status
+    int32_t *d_work = nullptr;     // kWorkInts ints (above)
     int64_t work_n = 0;
+    int32_t *d_lists = nullptr;    // per-query ef: the queries of each list width class
+    int64_t lists_n = 0;
     int32_t *d_cand = nullptr;     // the walk's final lists, nq * 32 * slots ids
     int64_t cand_n = 0;
     uint8_t *d_fq = nullptr, *d_tq = nullptr;
@@ -832,17 +841,17 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
     if (ef > pk::kFastMaxEf) return fail(PK_ERR_ARG, "ef too large for the fast path (max 512)");
     PK_TRY(refresh_traversal(h));
-    int slots = 1;
-    while (32 * slots < ef) slots *= 2;
+    const int slots = pk::list_slots(ef);
     const int cs = 32 * slots;
+    // per-query ef: queries are binned by list width and each width runs in
+    // its own launch, so a query pays for the list it needs
+    const bool binned = ef_arr != nullptr && slots > 1;
     WalkShape ws;
     PK_TRY(walk_shape(h, ws));
     const pk::TravCfgHost tc = pk::trav_config(h->trav_row_bytes, h->trav);
-    const int nb = pk::walk_blocks_per_sm(h->trav, tc, slots, ws.wpb, ws.smem);
-    if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
-    const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + ws.wpb - 1) / ws.wpb);
-    PK_TRY(ensure_buf(h, &c.d_work, c.work_n, 2));
+    PK_TRY(ensure_buf(h, &c.d_work, c.work_n, kWorkInts));
     PK_TRY(ensure_buf(h, &c.d_cand, c.cand_n, nq * cs));
+    if (binned) PK_TRY(ensure_buf(h, &c.d_lists, c.lists_n, nq * pk::kSlotClasses));
     // exact queries (padded rows) and traversal queries
     const size_t w = (size_t)(h->dim * h->esz);
     const uint8_t *qx = static_cast<const uint8_t *>(queries);
@@ -858,14 +867,15 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     PK_TRY(ensure_buf(h, &c.d_qn, c.qn_n, nq));
     PK_CUDA(pk::launch_prep_queries(h->dtype, h->trav, qx, h->row_bytes, nq, (int)h->dim, h->d_scale, c.d_tq, tq_rb,
                                     c.d_qn, s));
-    PK_CUDA(cudaMemsetAsync(c.d_work, 0, sizeof(int32_t) * 2, s));
+    PK_CUDA(cudaMemsetAsync(c.d_work, 0, sizeof(int32_t) * kWorkInts, s));
+    if (binned) PK_CUDA(pk::launch_bin_by_slots(ef_arr, ef, nq, c.d_work + kWorkCounts, c.d_lists, s));
     pk::WalkArgs a{};
     a.nq = nq;
     a.ef = ef;
     a.expand = std::max(1, std::min(4, expand > 0 ? expand : 1));
     a.ef_arr = ef_arr;
     a.counters = counters;
-    a.work = c.d_work;
+    a.status = c.d_work + kWorkStatus;
     a.cand = c.d_cand;
     a.cand_stride = cs;
     a.rb = ws.rb;
@@ -884,7 +894,17 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
             if (!e) PK_CUDA(cudaEventCreate(&e));
         PK_CUDA(cudaEventRecord(c.ev[0], s));
     }
-    PK_CUDA(pk::launch_walk(h->dg, h->trav, tc, slots, a, (int)grid, ws.wpb, ws.smem, s));
+    for (int cls = 0; (1 << cls) <= slots; cls++) {
+        const int sl = 1 << cls;
+        if (!binned && sl != slots) continue;
+        const int nb = pk::walk_blocks_per_sm(h->trav, tc, sl, ws.wpb, ws.smem);
+        if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
+        const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + ws.wpb - 1) / ws.wpb);
+        a.work = c.d_work + kWorkCounters + cls;
+        a.qlist = binned ? c.d_lists + cls * nq : nullptr;
+        a.qcount = binned ? c.d_work + kWorkCounts + cls : nullptr;
+        PK_CUDA(pk::launch_walk(h->dg, h->trav, tc, sl, a, (int)grid, ws.wpb, ws.smem, s));
+    }
     if (timed) PK_CUDA(cudaEventRecord(c.ev[1], s));
 
     int rwpb = 4;
@@ -908,7 +928,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     r.out_dists = dists;
     r.ext0 = h->hg.L[0].ext;
     r.cand = c.d_cand;
-    r.status = c.d_work + 1;
+    r.status = c.d_work + kWorkStatus;
     r.queries = qx;
     r.row_bytes = h->row_bytes;
     PK_CUDA(pk::launch_rerank(h->dg, h->dtype, h->lc, r, (int)rgrid, rwpb, rsmem, s));
@@ -919,7 +939,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
 // After a synchronised fast search: the walk's status.
 int fast_status(pk_index *h, FastCtx &c, cudaStream_t s) {
     int32_t st = 0;
-    PK_CUDA(cudaMemcpyAsync(&st, c.d_work + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaMemcpyAsync(&st, c.d_work + kWorkStatus, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PK_CUDA(cudaStreamSynchronize(s));
     if (st != 0) return fail(PK_ERR_TIMEOUT, "a row fetch of the fast search did not complete in time");
     return PK_OK;
@@ -971,6 +991,7 @@ void free_fast_ctx(pk_index *h, FastCtx &c) {
         if (e) cudaEventDestroy(e);
     dfree(h, c.d_work, 4 * (size_t)c.work_n);
     dfree(h, c.d_cand, 4 * (size_t)c.cand_n);
+    dfree(h, c.d_lists, 4 * (size_t)c.lists_n);
     dfree(h, c.d_fq, (size_t)c.fq_n);
     dfree(h, c.d_tq, (size_t)c.tq_n);
     dfree(h, c.d_qn, 4 * (size_t)c.qn_n);
@@ -1633,7 +1654,7 @@ void srv_loop(pk_server *S) {
                                      sl.stream) != cudaSuccess ||
                      cudaMemcpyAsync(sl.h_d, sl.d_d, 4 * (size_t)nq * S->max_k, cudaMemcpyDeviceToHost, sl.stream) !=
                          cudaSuccess ||
-                     cudaMemcpyAsync(sl.h_status, sl.ctx.d_work + 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                     cudaMemcpyAsync(sl.h_status, sl.ctx.d_work + kWorkStatus, sizeof(int32_t), cudaMemcpyDeviceToHost,
                                      sl.stream) != cudaSuccess ||
                      cudaEventRecord(sl.ev, sl.stream) != cudaSuccess))
                     rc = PK_ERR_CUDA;
