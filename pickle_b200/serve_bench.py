@@ -20,23 +20,6 @@ import time
 import numpy as np
 
 
-def gt_torch(base, queries, k, metric, device):
-    import torch
-    torch.backends.cuda.matmul.allow_tf32 = False
-    b = torch.from_numpy(base).to(device).float()
-    out = np.empty((len(queries), k), np.int64)
-    bn = (b * b).sum(1) if metric == "l2" else None
-    for i in range(0, len(queries), 512):
-        q = torch.from_numpy(queries[i:i + 512]).to(device).float()
-        s = -(q @ b.T) if metric == "ip" else (q * q).sum(1)[:, None] + bn[None, :] - 2 * q @ b.T
-        top = torch.topk(s, k + 32, dim=1, largest=False).indices
-        qd, bd = q.double(), b[top].double()
-        s64 = -(qd[:, None, :] * bd).sum(-1) if metric == "ip" else ((qd[:, None, :] - bd) ** 2).sum(-1)
-        order = torch.argsort(s64, dim=1, stable=True)[:, :k]
-        out[i:i + 512] = torch.gather(top, 1, order).cpu().numpy()
-    return out
-
-
 def main(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--config", default="c2", choices=["c2", "c5"])
@@ -55,6 +38,7 @@ def main(argv=None):
     import torch
 
     from pickle_b200 import HNSWIndex, Server, datasets
+    from pickle_b200.groundtruth import gpu_knn
     if a.config == "c2":
         n, dim, metric, M, efc = a.n or 1_000_000, 96, "ip", a.M or 32, a.efc or 400
         base, _ = datasets.gmm_unit(n, 0, dim, ncomp=256, sigma=0.3, seed=a.seed)
@@ -69,7 +53,7 @@ def main(argv=None):
     idx.build(base)
     build_s = time.time() - t0
     idx.prepare_fast(a.traversal)
-    gt = gt_torch(base, pool, 10, metric, torch.device("cuda"))
+    gt = gpu_knn(base, pool, 10, metric, torch.device("cuda"))
     srv = Server(idx, a.traversal, slots=a.slots, max_batch=a.max_batch, max_k=100, max_ef=256)
     rng = np.random.default_rng(a.seed + 1)
     for rate in [float(x) for x in a.rates.split(",")]:
