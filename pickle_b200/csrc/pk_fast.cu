@@ -17,8 +17,8 @@
 //   * on layer 0 the result set is a sorted list of ef entries held in
 //     registers (lane l owns entries l*S .. l*S+S-1); each iteration expands
 //     the `expand` best unexpanded entries, filters their neighbours through
-//     a small table of recently seen ids in shared memory (2-way sets,
-//     least recently inserted out),
+//     a table of recently seen ids in shared memory (exact 16-bit tags in
+//     4-way sets where the ids allow, least recently inserted out),
 //     fetches the new rows with one bulk copy (cp.async.bulk) per row onto a
 //     per-warp mbarrier, and inserts what beats the worst listed entry;
 //   * the walk ends when the first ef entries are all expanded, and their
@@ -259,6 +259,47 @@ __device__ __forceinline__ bool append_pending(bool ok, int32_t id, int32_t row,
     return true;
 }
 
+// ----------------------------------------------------- recently-seen ids --
+// Per-warp table in shared memory of 2^hlog2 id slots.  Exact 16-bit tags
+// where they fit: the id is scrambled by a bijection of [0, 2^B) (odd
+// multiplier, B = the ids' bits), the top bits pick a 4-way set of 8 bytes and
+// the remaining B - (hlog2 - 2) <= 15 bits, plus one, are the tag - distinct
+// ids never share a (set, tag), so a hit is always a real revisit.  Larger id
+// spaces use 2-way sets of 32-bit ids.  Either way the most recent id goes
+// first and the oldest of a full set is forgotten.
+struct SeenTable {
+    uint32_t *w;
+    int words;        // 32-bit words of the table
+    bool tag16;
+    uint32_t bmask;   // tag16: 2^B - 1
+    int tshift;       // tag16: B - set bits (the tag's width)
+    int sshift;       // 32-bit ids: 33 - hlog2
+
+    __device__ __forceinline__ void clear(int lane) {
+        const int4 fill = tag16 ? make_int4(0, 0, 0, 0) : make_int4(-1, -1, -1, -1);
+        for (int i = lane * 4; i < words; i += 128) *reinterpret_cast<int4 *>(w + i) = fill;
+    }
+
+    // Marks v as seen; true if it was not in the table.
+    __device__ __forceinline__ bool test_and_mark(int32_t v) {
+        if (tag16) {
+            const uint32_t h = ((uint32_t)v * 2654435761u) & bmask;
+            uint2 *set = reinterpret_cast<uint2 *>(w) + (h >> tshift);
+            const uint32_t tag = (h & ((1u << tshift) - 1u)) + 1u;
+            const uint2 x = *set;
+            const uint32_t t2 = tag * 0x10001u;
+            if ((__vcmpeq2(x.x, t2) | __vcmpeq2(x.y, t2)) != 0u) return false;
+            *set = make_uint2((x.x << 16) | tag, (x.y << 16) | (x.x >> 16));
+            return true;
+        }
+        int2 *set = reinterpret_cast<int2 *>(w) + (((uint32_t)v * 2654435769u) >> sshift);
+        const int2 x = *set;
+        if (x.x == v || x.y == v) return false;
+        *set = make_int2(v, x.x);
+        return true;
+    }
+};
+
 // ------------------------------------------------------------ result list --
 // The ef best entries found so far, sorted by (distance, id), in registers:
 // lane l holds entries l*S .. l*S+S-1.  Empty slots hold (+inf, kEmpty); the
@@ -388,9 +429,15 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const WalkLayout lay = walk_layout(a.rb, a.trav_row_bytes, a.hlog2);
+    const WalkLayout lay = walk_layout(a.rb, a.trav_row_bytes, a.hlog2, a.tag16 != 0);
     unsigned char *my = smem + (size_t)wib * lay.total;
-    int32_t *tab = reinterpret_cast<int32_t *>(my + lay.tab);
+    SeenTable seen;
+    seen.w = reinterpret_cast<uint32_t *>(my + lay.tab);
+    seen.tag16 = a.tag16 != 0;
+    seen.words = seen.tag16 ? (1 << (a.hlog2 - 1)) : (1 << a.hlog2);
+    seen.bmask = a.idbits >= 32 ? 0xffffffffu : (1u << a.idbits) - 1u;
+    seen.tshift = a.idbits - (a.hlog2 - 2);
+    seen.sshift = 33 - a.hlog2;
     int32_t *crow = reinterpret_cast<int32_t *>(my + lay.crow);
     int32_t *cid = reinterpret_cast<int32_t *>(my + lay.cid);
     float *cd = reinterpret_cast<float *>(my + lay.cd);
@@ -405,8 +452,6 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
     float *const norm_out = ip ? nullptr : cd;
     const int enter_level = gp->enter_level;
     const int rb = a.rb;
-    const int H = 1 << a.hlog2;
-    const int sshift = 33 - a.hlog2;  // 2^(hlog2 - 1) sets of two slots
     const int expand = max(1, min(a.expand, 4));
     const DevLayer L0 = gp->L[0];
     const int64_t lim0 = min(L0.lcap, a.trav_rows);
@@ -512,8 +557,8 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
         float wd = kInf;
         uint32_t wi = kEmpty & ~kExpanded;
         if (!failed) {
-            for (int i = lane * 4; i < H; i += 128)
-                *reinterpret_cast<int4 *>(tab + i) = make_int4(-1, -1, -1, -1);
+            seen.clear(lane);
+            __syncwarp();
             if (enter < 0 || enter >= lim0) enter = 0;
             if (lane == 0) crow[0] = enter;
             if (!fetch_rows(f, tv, crow, 1, norm_out, lane)) failed = true;
@@ -524,7 +569,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             if (lane == 0) {
                 list.d[0] = d0;
                 list.id[0] = (uint32_t)enter;
-                reinterpret_cast<int2 *>(tab)[((uint32_t)enter * 2654435769u) >> sshift] = make_int2(enter, -1);
+                seen.test_and_mark(enter);
             }
             __syncwarp();
             list.at(wl, wsl, wd, wi, lane);
@@ -588,16 +633,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                     const int j = j0 + lane;
                     int32_t v = -1;
                     if (j < deg) v = (j < L0.cap && j0 == 0) ? pa0[p] : (j < L0.cap && j0 == 32) ? pa1[p] : L0.adj[base + j];
-                    bool fresh = false;
-                    if (v >= 0 && v < lim0) {
-                        // 2-way set of the table: the most recent id first
-                        int2 *set = reinterpret_cast<int2 *>(tab) + (((uint32_t)v * 2654435769u) >> sshift);
-                        const int2 w = *set;
-                        if (w.x != v && w.y != v) {
-                            *set = make_int2(v, w.x);
-                            fresh = true;
-                        }
-                    }
+                    const bool fresh = v >= 0 && v < lim0 && seen.test_and_mark(v);
                     if (!append_pending(fresh, v, v, crow, cid, n, rb, lane, flush0)) {
                         failed = true;
                         break;

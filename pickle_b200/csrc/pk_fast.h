@@ -29,8 +29,9 @@ struct WalkArgs {
     int32_t *cand;              // nq * cand_stride: each query's final list (ids, -1 = empty)
     int32_t cand_stride;        // 32 * list slots per lane
     int32_t rb;                 // rows per fetch batch
-    int32_t hlog2;              // log2 of the visited-filter slots
-    int32_t pad_;
+    int32_t hlog2;              // log2 of the recently-seen table's id slots
+    int32_t tag16;              // 1: 16-bit tags in 4-way sets, 0: 32-bit ids in 2-way sets
+    int32_t idbits;             // bits of the largest node id (tag16)
     const uint8_t *tq_rows;     // traversal queries
     int64_t tq_row_bytes;
     const float *qnorm;         // sum of squares of each traversal query (L2)
@@ -48,21 +49,33 @@ __host__ __device__ inline int64_t stage_stride(int64_t trav_row_bytes) {
     return ((trav_row_bytes / 16) & 1) ? trav_row_bytes : trav_row_bytes + 16;
 }
 
+// Exact 16-bit tags fit when an id's bits beyond the set index (4-way sets:
+// hlog2 - 2 index bits) are at most 15.  idbits_for(n) = bits of ids below n.
+__host__ __device__ inline int idbits_for(int64_t n) {
+    int b = 1;
+    while (b < 32 && ((int64_t)1 << b) < n) b++;
+    return b;
+}
+__host__ __device__ inline bool seen_tag16(int64_t n, int hlog2) {
+    const int b = idbits_for(n) > hlog2 - 2 ? idbits_for(n) : hlog2 - 2;
+    return b - (hlog2 - 2) <= 15;
+}
+
 // Shared memory of one walk warp: the staged rows (rb rows, stride apart),
-// the query in the traversal format, the visited filter, the pending batch
+// the query in the traversal format, the recently-seen table, the pending batch
 // (rows, ids, distances), the mbarrier.  Every region starts on a 16-byte
 // boundary (bulk copies land on 16-byte boundaries).
 struct WalkLayout {
     int rowbuf, qbuf, tab, crow, cid, cd, bar, total;
     int64_t stride;
 };
-__host__ __device__ inline WalkLayout walk_layout(int rb, int64_t trav_row_bytes, int hlog2) {
+__host__ __device__ inline WalkLayout walk_layout(int rb, int64_t trav_row_bytes, int hlog2, bool tag16) {
     WalkLayout w;
     w.stride = stage_stride(trav_row_bytes);
     w.rowbuf = 0;
     w.qbuf = align16((int64_t)rb * w.stride);
     w.tab = w.qbuf + align16(trav_row_bytes);
-    w.crow = w.tab + (4 << hlog2);
+    w.crow = w.tab + ((tag16 ? 2 : 4) << hlog2);
     w.cid = w.crow + align16(4 * (int64_t)rb);
     w.cd = w.cid + align16(4 * (int64_t)rb);
     w.bar = w.cd + align16(4 * (int64_t)rb);

@@ -817,6 +817,8 @@ int refresh_traversal(pk_index *h) {
 // filter size, warps per block, and the shared memory that takes.
 struct WalkShape {
     int rb, hlog2, wpb;
+    bool tag16;
+    int idbits;
     size_t smem;
 };
 int walk_shape(const pk_index *h, WalkShape &w) {
@@ -824,10 +826,13 @@ int walk_shape(const pk_index *h, WalkShape &w) {
     w.rb = h->fast_rb > 0 ? h->fast_rb : (int)std::max<int64_t>(8, std::min<int64_t>(32, 12288 / trb));
     w.hlog2 = h->fast_hlog2 > 0 ? h->fast_hlog2 : 9;
     w.wpb = h->fast_wpb > 0 ? h->fast_wpb : 4;
-    w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2).total;
+    const int64_t ids = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
+    w.tag16 = pk::seen_tag16(ids, w.hlog2);
+    w.idbits = std::max(pk::idbits_for(ids), w.hlog2 - 2);
+    w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2, w.tag16).total;
     while (w.wpb > 1 && w.smem > 200 * 1024) {
         w.wpb /= 2;
-        w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2).total;
+        w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2, w.tag16).total;
     }
     if (w.smem > 227 * 1024) return fail(PK_ERR_ARG, "walk working set exceeds shared memory: lower rows or filter bits");
     return PK_OK;
@@ -880,6 +885,8 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     a.cand_stride = cs;
     a.rb = ws.rb;
     a.hlog2 = ws.hlog2;
+    a.tag16 = ws.tag16 ? 1 : 0;
+    a.idbits = ws.idbits;
     a.tq_rows = c.d_tq;
     a.tq_row_bytes = tq_rb;
     a.qnorm = c.d_qn;

@@ -218,3 +218,21 @@ def test_fast_timing_events(gpu, ref_bin):
     idx.search_fast(queries, 10, 48)
     walk_ms, rerank_ms = idx.fast_timing()
     assert walk_ms > 0 and rerank_ms > 0
+
+
+def test_seen_table_layouts_agree(gpu):
+    """300k node ids: a 32-slot table cannot hold exact 16-bit tags for them
+    (18 id bits beyond 3 set bits) and uses 32-bit ids; a 4096-slot table
+    uses tags.  Both are only caches of visited ids: same results."""
+    base, queries = datasets.gmm_unit(300_000, 200, 16, ncomp=64, seed=9)
+    idx = HNSWIndex(16, np.float32, "ip", M=8, ef_construction=32)
+    idx.build(base)
+    idx.prepare_fast("f16")
+    idx.set_fast_params(32, 5, 4)
+    a_i, a_d = idx.search_fast(queries, 10, 64)
+    idx.set_fast_params(32, 12, 4)
+    b_i, b_d = idx.search_fast(queries, 10, 64)
+    np.testing.assert_array_equal(a_i, b_i)
+    np.testing.assert_array_equal(a_d, b_d)
+    gt, _ = datasets.exact_knn(base, queries, 10, "ip")
+    assert datasets.recall_at_k(a_i, gt, 10) >= 0.9
