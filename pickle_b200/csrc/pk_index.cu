@@ -824,7 +824,7 @@ struct WalkShape {
 int walk_shape(const pk_index *h, WalkShape &w) {
     const int64_t trb = h->trav_row_bytes;
     w.rb = h->fast_rb > 0 ? h->fast_rb : (int)std::max<int64_t>(8, std::min<int64_t>(32, 12288 / trb));
-    w.hlog2 = h->fast_hlog2 > 0 ? h->fast_hlog2 : 9;
+    w.hlog2 = h->fast_hlog2 > 0 ? h->fast_hlog2 : 10;
     w.wpb = h->fast_wpb > 0 ? h->fast_wpb : 4;
     const int64_t ids = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
     w.tag16 = pk::seen_tag16(ids, w.hlog2);
