@@ -77,12 +77,6 @@ cudaError_t fill_f32(float *p, int64_t n, float v, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-int64_t pow2ceil(int64_t x) {
-    int64_t p = 1;
-    while (p < x) p <<= 1;
-    return p;
-}
-
 // splitmix64: the per-node random stream of the level draw.
 inline uint64_t splitmix64(uint64_t &s) {
     uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
