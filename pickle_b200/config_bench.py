@@ -121,6 +121,9 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--cpu-sample", type=int, default=0, help="queries timed on the reference's CPU search")
+    p.add_argument("--efs", default="", help="comma-separated ef list instead of the configuration's sweep")
+    p.add_argument("--no-mixed", action="store_true", help="skip the mixed k/ef batch")
+    p.add_argument("--fast-shape", default="", help="rows,filter_log2,warps for the fast walk instead of tuning")
     a = p.parse_args(argv)
 
     import torch
@@ -141,7 +144,8 @@ def main(argv=None):
     build_s = time.time() - t0
     info = idx.info()
     dev = torch.device("cuda")
-    mixed = c.get("mixed", False)
+    mixed = c.get("mixed", False) and not a.no_mixed
+    ef_list = [int(x) for x in a.efs.split(",")] if a.efs else c["efs"]
     kmax = 100 if mixed else 10
     t0 = time.time()
     gt = gpu_knn(base, queries, kmax, c["metric"], dev)
@@ -161,7 +165,7 @@ def main(argv=None):
         efq = np.array([rng.integers(max(int(k), 16), 513) for k in kq], np.int32)
         runs.append(("mixed", int(kq.max()), int(efq.max()), kq, torch.from_numpy(kq).to(dev),
                      torch.from_numpy(efq).to(dev)))
-    runs += [(str(e), 10, e, k10, None, None) for e in c["efs"]]
+    runs += [(str(e), 10, e, k10, None, None) for e in ef_list]
     stride = max(r[1] for r in runs)
     ids = torch.empty((nq, stride), dtype=torch.int32, device=dev)
     ds = torch.empty((nq, stride), dtype=torch.float32, device=dev)
@@ -182,7 +186,11 @@ def main(argv=None):
                 continue
             shape = None
             if path != "exact":
-                shape, _ = idx.tune_fast(q, k, min(ef, 512))
+                if a.fast_shape:
+                    shape = tuple(int(x) for x in a.fast_shape.split(","))
+                    idx.set_fast_params(*shape)
+                else:
+                    shape, _ = idx.tune_fast(q, k, min(ef, 512))
             call(path, k, ef, k_dev, ef_dev)
             torch.cuda.synchronize()
             times = []
