@@ -105,7 +105,15 @@ struct TravView {
 // by as many lanes as there are rows and completing on a per-warp mbarrier
 // that counts the bytes.  A warp waits once per batch of rows.
 
-constexpr int kWaitPolls = 1 << 20;  // bound on mbarrier polls for one batch
+// Bound on the wait for one batch of rows: 2 s of the global timer (a batch
+// lands in microseconds), checked every 64 polls.
+constexpr uint64_t kWaitNs = 2000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -136,7 +144,7 @@ struct RowFetch {
 // Copies rows[0..n) of the traversal copy (n >= 1; each a row index below the
 // copy's row count, or -1 for the zero row) into f.buf.  With norm_out, the
 // rows' stored norms go to norm_out[t].  All lanes call.  Returns false on
-// every lane if the copies did not land within the poll bound; the copies are
+// every lane if the copies did not land within the time bound; the copies are
 // then given one more bounded wait before returning.
 __device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, const int32_t *rows, int n,
                                            float *norm_out, int lane) {
@@ -156,11 +164,22 @@ __device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, cons
             : "memory");
         if (norm_out) norm_out[t] = r >= 0 ? tv.rownorm[r] : 0.f;
     }
-    bool ok = false;
-    for (int i = 0; i < kWaitPolls && !ok; i++) ok = mbar_poll(f.bar, f.parity);
+    bool ok = mbar_poll(f.bar, f.parity);
+    if (!ok) {
+        const uint64_t t0 = global_ns();
+        for (int i = 1; !ok; i++) {
+            ok = mbar_poll(f.bar, f.parity);
+            if (!ok && (i & 63) == 0 && global_ns() - t0 > kWaitNs) break;
+        }
+    }
     const bool all = __all_sync(kFull, ok);
-    if (!all && !ok)
-        for (int i = 0; i < kWaitPolls && !ok; i++) ok = mbar_poll(f.bar, f.parity);
+    if (!all && !ok) {
+        const uint64_t t0 = global_ns();
+        for (int i = 1; !ok; i++) {
+            ok = mbar_poll(f.bar, f.parity);
+            if (!ok && (i & 63) == 0 && global_ns() - t0 > kWaitNs) break;
+        }
+    }
     f.parity ^= 1u;
     __syncwarp();
     return all;

@@ -1398,6 +1398,8 @@ static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq,
                 rc = fail(PK_ERR_CUDA, "cudaEventElapsedTime failed");
             if (rep > 0) ms += t;
         }
+        // a walk that stopped early on a fetch timeout must not look fast
+        if (rc == PK_OK) rc = fast_status(h, h->fctx, s);
         if (rc != PK_OK) return false;
         ms /= 2.f;
         if (best < 0.f || ms < best) {
