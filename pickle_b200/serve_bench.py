@@ -54,6 +54,8 @@ def main(argv=None):
     build_s = time.time() - t0
     idx.prepare_fast(a.traversal)
     gt = gpu_knn(base, pool, 10, metric, torch.device("cuda"))
+    # the walk's launch shape, tuned on a full batch of pool queries at the stream's middle ef
+    shape, _ = idx.tune_fast(torch.from_numpy(pool[:a.max_batch]).cuda(), 50, 144)
     srv = Server(idx, a.traversal, slots=a.slots, max_batch=a.max_batch, max_k=100, max_ef=256)
     rng = np.random.default_rng(a.seed + 1)
     for rate in [float(x) for x in a.rates.split(",")]:
@@ -70,6 +72,7 @@ def main(argv=None):
         print(json.dumps({
             "config": a.config, "n": n, "dim": dim, "metric": metric, "M": M, "ef_construction": efc,
             "traversal": a.traversal, "slots": a.slots, "max_batch": a.max_batch, "build_s": round(build_s, 1),
+            "launch_shape": shape,
             "offered_req_per_s": rate, "requests": nreq, "served_req_per_s": round(nreq / (span_ms / 1e3), 1),
             "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
                            "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3)},
