@@ -2,9 +2,11 @@
 
     python -m pickle_b200.serve_bench [--config c2|c5] [--n N] [--rates 20000,50000,...] [--duration 2]
 
-Each request is one query with k uniform in {10, 50, 100} and ef uniform in
-[max(k, 32), 256]; arrivals are a Poisson process at each rate (requests per
-second).  The stream is replayed by the library's native replayer
+Each request is one query with k uniform in {10, 50, 100}; arrivals are a
+Poisson process at each rate (requests per second).  Two streams per rate:
+"mixed", ef uniform in [max(k, 32), 256] (the configuration's range), and
+"target", ef = max(k, ef95) where ef95 is the smallest ef of a sweep whose
+recall@10 on the query pool (k = 10, one batch) is >= 0.95.  The stream is replayed by the library's native replayer
 (pk_server_replay) against a continuous-batching server (slots overlapping on
 the GPU, batches of up to --max-batch queries).  Reported per rate: offered
 and served requests/s, p50/p99/max latency (submit to results on the host)
@@ -33,6 +35,7 @@ def main(argv=None):
     p.add_argument("--M", type=int, default=0)
     p.add_argument("--efc", type=int, default=0)
     p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--streams", default="mixed,target")
     a = p.parse_args(argv)
 
     import torch
@@ -56,28 +59,45 @@ def main(argv=None):
     gt = gpu_knn(base, pool, 10, metric, torch.device("cuda"))
     # the walk's launch shape, tuned on a full batch of pool queries at the stream's middle ef
     shape, _ = idx.tune_fast(torch.from_numpy(pool[:a.max_batch]).cuda(), 50, 144)
-    srv = Server(idx, a.traversal, slots=a.slots, max_batch=a.max_batch, max_k=100, max_ef=256)
+    # recall@10 of the pool at k = 10 over an ef sweep: the stream at the target
+    sweep = {}
+    ef95 = 512
+    for e in [64, 96, 128, 192, 256, 384, 512]:
+        fi, _ = idx.search_fast(pool, 10, e)
+        sweep[e] = round(datasets.recall_at_k(fi, gt, 10), 4)
+        if sweep[e] >= 0.95:
+            ef95 = e
+            break
+    print(json.dumps({"config": a.config, "event": "ef_sweep", "k": 10, "recall_at_10": sweep, "ef95": ef95}),
+          flush=True)
+    srv = Server(idx, a.traversal, slots=a.slots, max_batch=a.max_batch, max_k=100, max_ef=512)
     rng = np.random.default_rng(a.seed + 1)
-    for rate in [float(x) for x in a.rates.split(",")]:
-        nreq = max(1, int(rate * a.duration))
-        arrival = np.cumsum(rng.exponential(1e6 / rate, size=nreq))
-        sel = rng.integers(0, len(pool), size=nreq)
-        k = rng.choice([10, 50, 100], size=nreq).astype(np.int32)
-        ef = np.array([rng.integers(max(kk, 32), 257) for kk in k], np.int32)
-        ids, _, lat = srv.replay(pool[sel], np.ones(nreq, np.int32), arrival, k, ef, out_stride=100)
-        done = arrival / 1e3 + lat
-        span_ms = done.max() - arrival[0] / 1e3
-        rec = datasets.recall_at_k(ids[:, :10], gt[sel], 10)
-        st = srv.stats()
-        print(json.dumps({
-            "config": a.config, "n": n, "dim": dim, "metric": metric, "M": M, "ef_construction": efc,
-            "traversal": a.traversal, "slots": a.slots, "max_batch": a.max_batch, "build_s": round(build_s, 1),
-            "launch_shape": shape,
-            "offered_req_per_s": rate, "requests": nreq, "served_req_per_s": round(nreq / (span_ms / 1e3), 1),
-            "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
-                           "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3)},
-            "recall_at_10": round(rec, 4), "k": "uniform {10,50,100}", "ef": "uniform [max(k,32), 256]",
-            "server": st}), flush=True)
+    for stream in a.streams.split(","):
+        for rate in [float(x) for x in a.rates.split(",")]:
+            nreq = max(1, int(rate * a.duration))
+            arrival = np.cumsum(rng.exponential(1e6 / rate, size=nreq))
+            sel = rng.integers(0, len(pool), size=nreq)
+            k = rng.choice([10, 50, 100], size=nreq).astype(np.int32)
+            if stream == "mixed":
+                ef = np.array([rng.integers(max(kk, 32), 257) for kk in k], np.int32)
+                ef_desc = "uniform [max(k,32), 256]"
+            else:
+                ef = np.maximum(k, ef95).astype(np.int32)
+                ef_desc = f"max(k, {ef95})"
+            ids, _, lat = srv.replay(pool[sel], np.ones(nreq, np.int32), arrival, k, ef, out_stride=100)
+            done = arrival / 1e3 + lat
+            span_ms = done.max() - arrival[0] / 1e3
+            rec = datasets.recall_at_k(ids[:, :10], gt[sel], 10)
+            st = srv.stats()
+            print(json.dumps({
+                "config": a.config, "n": n, "dim": dim, "metric": metric, "M": M, "ef_construction": efc,
+                "traversal": a.traversal, "slots": a.slots, "max_batch": a.max_batch, "build_s": round(build_s, 1),
+                "launch_shape": shape,
+                "offered_req_per_s": rate, "requests": nreq, "served_req_per_s": round(nreq / (span_ms / 1e3), 1),
+                "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                               "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3)},
+                "stream": stream, "recall_at_10": round(rec, 4), "k": "uniform {10,50,100}", "ef": ef_desc,
+                "server": st}), flush=True)
     srv.close()
 
 
