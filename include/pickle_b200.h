@@ -145,8 +145,8 @@ int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int3
                               float *out_dists, int32_t expand);
 
 /* Launch shape of pk_index_search_fast's walk (0 keeps the default):
- * rows_per_batch = vector rows per fetch batch, two batches in flight
- * (1..256; default min(16, 6 KiB / row)); filter_log2 = log2 of the slots of the per-query
+ * rows_per_batch = vector rows fetched per round trip (1..256; default
+ * min(32, 12 KiB / row)); filter_log2 = log2 of the slots of the per-query
  * table of recently seen ids (5..15; default 10); warps_per_block (1..8;
  * default 4).  The results do not depend on the shape (the table only saves
  * recomputed distances); the speed does.  No counterpart in the reference. */

@@ -134,65 +134,41 @@ __device__ __forceinline__ bool mbar_poll(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// The walk's two batch buffers.  Buffer b holds staged rows at buf(b) +
-// t * stride, the batch's row indices crow(b), node ids cid(b), distances (or,
-// for L2 before the distances, stored norms) cd(b), and the mbarrier bar(b)
-// its bulk copies complete on; bit b of parity is that mbarrier's phase.
-// Everything is addressed from bases, so a buffer number can be a run-time
-// value without the buffers leaving registers.
-struct Batches {
-    uint8_t *buf0;
-    int buf_step;        // bytes between the two row buffers
-    int32_t *crow0, *cid0;
-    float *cd0;
-    int int_step;        // 32-bit words between the two buffers' arrays
-    uint64_t *bar0;
+struct RowFetch {
+    uint8_t *buf;    // row t lands at buf + t * stride
+    int64_t stride;
+    uint64_t *bar;
     uint32_t parity;
-    __device__ __forceinline__ uint8_t *buf(int b) const { return buf0 + b * buf_step; }
-    __device__ __forceinline__ int32_t *crow(int b) const { return crow0 + b * int_step; }
-    __device__ __forceinline__ int32_t *cid(int b) const { return cid0 + b * int_step; }
-    __device__ __forceinline__ float *cd(int b) const { return cd0 + b * int_step; }
-    __device__ __forceinline__ uint64_t *bar(int b) const { return bar0 + b; }
 };
 
-// Issues the bulk copies of buffer b's rows crow(b)[0..n) of the traversal
-// copy (n >= 1; each a row index below the copy's row count, or -1 for the
-// zero row), without waiting.  With norms, the rows' stored norms go to
-// cd(b)[t].  All lanes call.
-__device__ __forceinline__ void issue_rows(const Batches &q, int b, int64_t stride, const TravView &tv, int n,
-                                           bool norms, int lane) {
-    uint8_t *buf = q.buf(b);
-    const int32_t *crow = q.crow(b);
-    float *cd = q.cd(b);
-    const uint32_t bar = smem_u32(q.bar(b));
+// Copies rows[0..n) of the traversal copy (n >= 1; each a row index below the
+// copy's row count, or -1 for the zero row) into f.buf.  With norm_out, the
+// rows' stored norms go to norm_out[t].  All lanes call.  Returns false on
+// every lane if the copies did not land within the time bound; the copies are
+// then given one more bounded wait before returning.
+__device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, const int32_t *rows, int n,
+                                           float *norm_out, int lane) {
     __syncwarp();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (lane == 0)
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(f.bar)),
                      "r"((uint32_t)(n * tv.row_bytes))
                      : "memory");
     __syncwarp();
     for (int t = lane; t < n; t += 32) {
-        const int32_t r = crow[t];
+        const int32_t r = rows[t];
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                smem_u32(buf + t * stride)),
-            "l"(tv.row(r)), "r"((uint32_t)tv.row_bytes), "r"(bar)
+                smem_u32(f.buf + t * f.stride)),
+            "l"(tv.row(r)), "r"((uint32_t)tv.row_bytes), "r"(smem_u32(f.bar))
             : "memory");
-        if (norms) cd[t] = r >= 0 ? tv.rownorm[r] : 0.f;
+        if (norm_out) norm_out[t] = r >= 0 ? tv.rownorm[r] : 0.f;
     }
-}
-
-// Waits for buffer b's copies.  Returns false on every lane if they did not
-// land within the time bound (after one more bounded wait).  All lanes call.
-__device__ __forceinline__ bool wait_rows(Batches &q, int b) {
-    uint64_t *bar = q.bar(b);
-    const uint32_t par = (q.parity >> b) & 1u;
-    bool ok = mbar_poll(bar, par);
+    bool ok = mbar_poll(f.bar, f.parity);
     if (!ok) {
         const uint64_t t0 = global_ns();
         for (int i = 1; !ok; i++) {
-            ok = mbar_poll(bar, par);
+            ok = mbar_poll(f.bar, f.parity);
             if (!ok && (i & 63) == 0 && global_ns() - t0 > kWaitNs) break;
         }
     }
@@ -200,19 +176,13 @@ __device__ __forceinline__ bool wait_rows(Batches &q, int b) {
     if (!all && !ok) {
         const uint64_t t0 = global_ns();
         for (int i = 1; !ok; i++) {
-            ok = mbar_poll(bar, par);
+            ok = mbar_poll(f.bar, f.parity);
             if (!ok && (i & 63) == 0 && global_ns() - t0 > kWaitNs) break;
         }
     }
-    q.parity ^= 1u << b;
+    f.parity ^= 1u;
     __syncwarp();
     return all;
-}
-
-__device__ __forceinline__ bool fetch_rows(Batches &q, int b, int64_t stride, const TravView &tv, int n, bool norms,
-                                           int lane) {
-    issue_rows(q, b, stride, tv, n, norms, lane);
-    return wait_rows(q, b);
 }
 
 // Traversal distances of the n staged rows to the query, into cd[t] (for L2,
@@ -227,14 +197,14 @@ __device__ __forceinline__ bool fetch_rows(Batches &q, int b, int64_t stride, co
 // E4M3: groups of G lanes per row, FP32 FMAs over the decoded elements.
 template <int TRAV, int KT>
 __device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery<TRAV, KT> &tq, bool ip, float qnorm,
-                                              const uint8_t *buf, int64_t stride, int64_t row_bytes,
-                                              const uint8_t *qbuf, float *cd, int n, int lane) {
+                                              const RowFetch &f, int64_t row_bytes, const uint8_t *qbuf, float *cd,
+                                              int n, int lane) {
     if constexpr (TRAV == kTravF16) {
         const int ks = (int)(row_bytes / 32);
         const uint32_t *qw = reinterpret_cast<const uint32_t *>(qbuf);
         for (int t0 = 0; t0 < n; t0 += 16) {
             const int r = min(t0 + (lane & 15), n - 1);
-            const uint32_t arow = smem_u32(buf + r * stride) + (uint32_t)(lane >> 4) * 16u;
+            const uint32_t arow = smem_u32(f.buf + r * f.stride) + (uint32_t)(lane >> 4) * 16u;
             float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
             for (int kk = 0; kk < ks; kk++) {
                 uint32_t a0, a1, a2, a3;
@@ -266,7 +236,7 @@ __device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery
             const int t = base + grp;
             float acc = 0.f;
             if (t < n) {
-                const uint8_t *row = buf + t * stride;
+                const uint8_t *row = f.buf + t * f.stride;
 #pragma unroll
                 for (int k = 0; k < KT; k++) {
                     const int c = gl + k * G;
@@ -281,12 +251,11 @@ __device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery
 }
 
 // Appends this warp's new entries (lanes with ok, in lane order) to the
-// pending batch crow/cid at n, flushing the batch whenever rb entries wait
-// (a flush may move crow/cid to another buffer).  Returns false if a flush
-// failed.
+// pending batch crow/cid at n, flushing the batch whenever rb entries wait.
+// Returns false if a flush failed.
 template <class Flush>
-__device__ __forceinline__ bool append_pending(bool ok, int32_t id, int32_t row, int32_t *&crow, int32_t *&cid,
-                                               int &n, int rb, int lane, Flush &flush) {
+__device__ __forceinline__ bool append_pending(bool ok, int32_t id, int32_t row, int32_t *crow, int32_t *cid, int &n,
+                                               int rb, int lane, Flush &flush) {
     const unsigned m = __ballot_sync(kFull, ok);
     const int total = __popc(m);
     const int rank = __popc(m & ((1u << lane) - 1u));
@@ -488,28 +457,18 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
     seen.bmask = a.idbits >= 32 ? 0xffffffffu : (1u << a.idbits) - 1u;
     seen.tshift = a.idbits - (a.hlog2 - 2);
     seen.sshift = 33 - a.hlog2;
-    // two batch buffers: while one batch's rows are in flight the walk
-    // computes and inserts the other's
-    Batches bt;
-    bt.buf0 = my + lay.rowbuf[0];
-    bt.buf_step = lay.rowbuf[1] - lay.rowbuf[0];
-    bt.crow0 = reinterpret_cast<int32_t *>(my + lay.crow[0]);
-    bt.cid0 = reinterpret_cast<int32_t *>(my + lay.cid[0]);
-    bt.cd0 = reinterpret_cast<float *>(my + lay.cd[0]);
-    bt.int_step = (lay.crow[1] - lay.crow[0]) / 4;
-    bt.bar0 = reinterpret_cast<uint64_t *>(my + lay.bar[0]);
-    bt.parity = 0u;
-    if (lane == 0) {
-        mbar_init(bt.bar(0));
-        mbar_init(bt.bar(1));
-    }
+    int32_t *crow = reinterpret_cast<int32_t *>(my + lay.crow);
+    int32_t *cid = reinterpret_cast<int32_t *>(my + lay.cid);
+    float *cd = reinterpret_cast<float *>(my + lay.cd);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(my + lay.bar);
+    if (lane == 0) mbar_init(bar);
     __syncwarp();
     uint8_t *qbuf = my + lay.qbuf;
-    const int64_t stride = lay.stride;
+    RowFetch f{my + lay.rowbuf, lay.stride, bar, 0u};
 
     const TravView tv{a.trav, a.trav_zero, a.trav_row_bytes, a.rownorm};
     const bool ip = gp->metric == PK_METRIC_IP;
-    const bool norms = !ip;
+    float *const norm_out = ip ? nullptr : cd;
     const int enter_level = gp->enter_level;
     const int rb = a.rb;
     const int expand = max(1, min(a.expand, 4));
@@ -563,25 +522,24 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                 const int32_t r = Ly.vrow[v];
                 return r < a.trav_rows ? r : -1;
             };
-            int32_t *ucrow = bt.crow(0), *ucid = bt.cid(0);
-            if (lane == 0) ucrow[0] = vrow(enter);
-            if (!fetch_rows(bt, 0, stride, tv, 1, norms, lane)) {
+            if (lane == 0) crow[0] = vrow(enter);
+            if (!fetch_rows(f, tv, crow, 1, norm_out, lane)) {
                 failed = true;
                 break;
             }
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, bt.buf(0), stride, tv.row_bytes, qbuf, bt.cd(0), 1, lane);
-            float best = bt.cd(0)[0];
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, 1, lane);
+            float best = cd[0];
             int32_t c = enter;
             bool moved = false;
             auto flush_up = [&](int nn) -> bool {
-                if (!fetch_rows(bt, 0, stride, tv, nn, norms, lane)) return false;
-                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, bt.buf(0), stride, tv.row_bytes, qbuf, bt.cd(0), nn, lane);
+                if (!fetch_rows(f, tv, crow, nn, norm_out, lane)) return false;
+                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, nn, lane);
                 float bd;
-                int bi;
-                warp_argmin(bt.cd(0), nn, bd, bi, lane);
+                int bt;
+                warp_argmin(cd, nn, bd, bt, lane);
                 if (bd < best) {
                     best = bd;
-                    c = bt.cid(0)[bi];
+                    c = cid[bt];
                     moved = true;
                 }
                 cnt[1] += nn;
@@ -600,7 +558,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                     const int32_t v = j < deg ? Ly.adj[base + j] : -1;
                     const bool ok = v >= 0 && v < Ly.lcap;
                     const int32_t r = ok ? vrow(v) : -1;
-                    if (!append_pending(ok, v, r, ucrow, ucid, n, rb, lane, flush_up)) failed = true;
+                    if (!append_pending(ok, v, r, crow, cid, n, rb, lane, flush_up)) failed = true;
                 }
                 if (!failed && n > 0 && !flush_up(n)) failed = true;
                 if (failed || !moved) break;
@@ -621,12 +579,12 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             seen.clear(lane);
             __syncwarp();
             if (enter < 0 || enter >= lim0) enter = 0;
-            if (lane == 0) bt.crow(0)[0] = enter;
-            if (!fetch_rows(bt, 0, stride, tv, 1, norms, lane)) failed = true;
+            if (lane == 0) crow[0] = enter;
+            if (!fetch_rows(f, tv, crow, 1, norm_out, lane)) failed = true;
         }
         if (!failed) {
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, bt.buf(0), stride, tv.row_bytes, qbuf, bt.cd(0), 1, lane);
-            const float d0 = bt.cd(0)[0];
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, 1, lane);
+            const float d0 = cd[0];
             if (lane == 0) {
                 list.d[0] = d0;
                 list.id[0] = (uint32_t)enter;
@@ -635,30 +593,17 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             __syncwarp();
             list.at(wl, wsl, wd, wi, lane);
         }
-        // batches of new rows: a full batch is issued and the walk goes on to
-        // complete the previous one (distances, then insertions) while the
-        // new batch's rows are in flight; batches complete in issue order, so
-        // the list sees the same insertions in the same order as one batch
-        // at a time
-        int cur = 0;                   // the buffer being filled
-        uint32_t inflight = 0;         // bit b: buffer b's batch is in flight
-        int batch_n0 = 0, batch_n1 = 0;
-        int32_t *crow = bt.crow(0), *cid = bt.cid(0);
-        auto complete = [&](int b) -> bool {
-            const int nn = b ? batch_n1 : batch_n0;
-            const float *bcd = bt.cd(b);
-            const int32_t *bcrow = bt.crow(b);
-            inflight &= ~(1u << b);
-            if (!wait_rows(bt, b)) return false;
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, bt.buf(b), stride, tv.row_bytes, qbuf, bt.cd(b), nn, lane);
+        auto flush0 = [&](int nn) -> bool {
+            if (!fetch_rows(f, tv, crow, nn, norm_out, lane)) return false;
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, nn, lane);
             cnt[4] += nn;
             for (int i0 = 0; i0 < nn; i0 += 32) {
                 const int i = i0 + lane;
                 float nd = kInf;
                 uint32_t nid = kEmpty;
                 if (i < nn) {
-                    nd = bcd[i];
-                    nid = (uint32_t)bcrow[i];
+                    nd = cd[i];
+                    nid = (uint32_t)crow[i];
                 }
                 unsigned m = __ballot_sync(kFull, i < nn && nd < kInf && key_less(nd, nid, wd, wi));
                 while (m) {
@@ -672,20 +617,6 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                 }
             }
             __syncwarp();
-            return true;
-        };
-        // the slot being filled holds nn rows: issue it, complete the other
-        // (older) batch if it is in flight, and fill the other slot next
-        auto flush0 = [&](int nn) -> bool {
-            issue_rows(bt, cur, stride, tv, nn, norms, lane);
-            inflight |= 1u << cur;
-            if (cur) batch_n1 = nn;
-            else batch_n0 = nn;
-            const int o = cur ^ 1;
-            if (((inflight >> o) & 1u) && !complete(o)) return false;
-            cur = o;
-            crow = bt.crow(cur);
-            cid = bt.cid(cur);
             return true;
         };
         int64_t iters = 0;
@@ -729,15 +660,9 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                 }
             }
             if (!failed && n > 0 && !flush0(n)) failed = true;
-            // the step's last batch completes before the next parent is chosen
-            if (!failed && ((inflight >> (cur ^ 1)) & 1u) && !complete(cur ^ 1)) failed = true;
         }
         if (failed) {
             if (lane == 0) atomicExch(a.status, 1);
-            // copies still in flight land (bounded wait) before the warp leaves
-#pragma unroll
-            for (int b = 0; b < 2; b++)
-                if ((inflight >> b) & 1u) wait_rows(bt, b);
             return;
         }
 

@@ -28,7 +28,7 @@ struct WalkArgs {
     const int32_t *qcount;      // their number, on the device (null: nq)
     int32_t *cand;              // nq * cand_stride: each query's final list (ids, -1 = empty)
     int32_t cand_stride;        // 32 * list slots per lane
-    int32_t rb;                 // rows per fetch batch (two batches in flight)
+    int32_t rb;                 // rows per fetch batch
     int32_t hlog2;              // log2 of the recently-seen table's id slots
     int32_t tag16;              // 1: 16-bit tags in 4-way sets, 0: 32-bit ids in 2-way sets
     int32_t idbits;             // bits of the largest node id (tag16)
@@ -61,33 +61,25 @@ __host__ __device__ inline bool seen_tag16(int64_t n, int hlog2) {
     return b - (hlog2 - 2) <= 15;
 }
 
-// Shared memory of one walk warp: two batch buffers (rb staged rows, stride
-// apart), the query in the traversal format, the recently-seen table, per
-// buffer the batch's rows, ids and distances, two mbarriers.  Every region
-// starts on a 16-byte boundary (bulk copies land on 16-byte boundaries).
+// Shared memory of one walk warp: the staged rows (rb rows, stride apart),
+// the query in the traversal format, the recently-seen table, the pending batch
+// (rows, ids, distances), the mbarrier.  Every region starts on a 16-byte
+// boundary (bulk copies land on 16-byte boundaries).
 struct WalkLayout {
-    int rowbuf[2], qbuf, tab, crow[2], cid[2], cd[2], bar[2], total;
+    int rowbuf, qbuf, tab, crow, cid, cd, bar, total;
     int64_t stride;
 };
 __host__ __device__ inline WalkLayout walk_layout(int rb, int64_t trav_row_bytes, int hlog2, bool tag16) {
     WalkLayout w;
     w.stride = stage_stride(trav_row_bytes);
-    const int rows = align16((int64_t)rb * w.stride);
-    w.rowbuf[0] = 0;
-    w.rowbuf[1] = rows;
-    w.qbuf = 2 * rows;
+    w.rowbuf = 0;
+    w.qbuf = align16((int64_t)rb * w.stride);
     w.tab = w.qbuf + align16(trav_row_bytes);
-    int off = w.tab + ((tag16 ? 2 : 4) << hlog2);
-    const int ints = align16(4 * (int64_t)rb);
-    for (int b = 0; b < 2; b++) {
-        w.crow[b] = off;
-        w.cid[b] = off + ints;
-        w.cd[b] = off + 2 * ints;
-        off += 3 * ints;
-    }
-    w.bar[0] = off;
-    w.bar[1] = off + 8;
-    w.total = off + 16;
+    w.crow = w.tab + ((tag16 ? 2 : 4) << hlog2);
+    w.cid = w.crow + align16(4 * (int64_t)rb);
+    w.cd = w.cid + align16(4 * (int64_t)rb);
+    w.bar = w.cd + align16(4 * (int64_t)rb);
+    w.total = w.bar + 16;
     return w;
 }
 

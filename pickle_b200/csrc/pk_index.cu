@@ -817,7 +817,7 @@ struct WalkShape {
 };
 int walk_shape(const pk_index *h, WalkShape &w) {
     const int64_t trb = h->trav_row_bytes;
-    w.rb = h->fast_rb > 0 ? h->fast_rb : (int)std::max<int64_t>(8, std::min<int64_t>(16, 6144 / trb));
+    w.rb = h->fast_rb > 0 ? h->fast_rb : (int)std::max<int64_t>(8, std::min<int64_t>(32, 12288 / trb));
     w.hlog2 = h->fast_hlog2 > 0 ? h->fast_hlog2 : 10;
     w.wpb = h->fast_wpb > 0 ? h->fast_wpb : 4;
     const int64_t ids = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
@@ -1410,16 +1410,16 @@ static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq,
         }
         return true;
     };
-    // stage 1: visited-table size and warps per block at 16 rows per batch
+    // stage 1: visited-table size and warps per block at 32 rows per batch
     // (the table trades re-fetched rows against occupancy, more so as ef
     // grows); stage 2: rows per batch at the best pair
     const int hls[] = {8, 9, 10, 11, 12, 13};
     const int wps[] = {1, 2, 4};
     for (int hl : hls)
         for (int wp : wps)
-            if (rc == PK_OK) time_shape(16, hl, wp);
+            if (rc == PK_OK) time_shape(32, hl, wp);
     const int h1 = bh, w1 = bw;
-    const int rbs[] = {8, 24, 32, 48};
+    const int rbs[] = {16, 24, 48, 64};
     for (int rb : rbs)
         if (rc == PK_OK && best >= 0.f) time_shape(rb, h1, w1);
     cudaEventDestroy(e0);
