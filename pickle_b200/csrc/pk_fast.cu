@@ -11,7 +11,8 @@
 //   * traversal distances come from a low-precision copy of the vectors:
 //     FP16 (dot products on the tensor cores), or FP8 E4M3 scaled per
 //     dimension (a query is scaled by the same per-dimension factors); for L2
-//     the stored per-row norms turn the distance into a dot product;
+//     each row carries its stored norm (after its values), which turns the
+//     distance into a dot product;
 //   * upper layers are descended greedily as in SlideLayer
 //     (include/hnsw.hpp:446-494);
 //   * on layer 0 the result set is a sorted list of ef entries held in
@@ -94,7 +95,6 @@ struct TravView {
     const uint8_t *rows;      // traversal copy, row_bytes apart
     const uint8_t *zero_row;
     int64_t row_bytes;
-    const float *rownorm;     // L2: sum of squares of the stored row's values
     __device__ __forceinline__ const uint8_t *row(int32_t r) const {
         return r >= 0 ? rows + (int64_t)r * row_bytes : zero_row;
     }
@@ -142,12 +142,10 @@ struct RowFetch {
 };
 
 // Copies rows[0..n) of the traversal copy (n >= 1; each a row index below the
-// copy's row count, or -1 for the zero row) into f.buf.  With norm_out, the
-// rows' stored norms go to norm_out[t].  All lanes call.  Returns false on
+// copy's row count, or -1 for the zero row) into f.buf.  All lanes call.  Returns false on
 // every lane if the copies did not land within the time bound; the copies are
 // then given one more bounded wait before returning.
-__device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, const int32_t *rows, int n,
-                                           float *norm_out, int lane) {
+__device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, const int32_t *rows, int n, int lane) {
     __syncwarp();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (lane == 0)
@@ -162,7 +160,6 @@ __device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, cons
                 smem_u32(f.buf + t * f.stride)),
             "l"(tv.row(r)), "r"((uint32_t)tv.row_bytes), "r"(smem_u32(f.bar))
             : "memory");
-        if (norm_out) norm_out[t] = r >= 0 ? tv.rownorm[r] : 0.f;
     }
     bool ok = mbar_poll(f.bar, f.parity);
     if (!ok) {
@@ -185,8 +182,9 @@ __device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, cons
     return all;
 }
 
-// Traversal distances of the n staged rows to the query, into cd[t] (for L2,
-// cd[t] holds the row's stored norm on entry).  All lanes call.
+// Traversal distances of the n staged rows to the query, into cd[t].  A row's
+// values take data_bytes; for L2 its stored norm (float) follows them.  All
+// lanes call.
 //
 // FP16: the tensor cores.  Sixteen staged rows at a time are the A operand of
 // mma.m16n8k16 (ldmatrix takes one row address per lane, so the gathered rows
@@ -197,10 +195,11 @@ __device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, cons
 // E4M3: groups of G lanes per row, FP32 FMAs over the decoded elements.
 template <int TRAV, int KT>
 __device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery<TRAV, KT> &tq, bool ip, float qnorm,
-                                              const RowFetch &f, int64_t row_bytes, const uint8_t *qbuf, float *cd,
+                                              const RowFetch &f, int64_t data_bytes, const uint8_t *qbuf, float *cd,
                                               int n, int lane) {
+    auto xnorm = [&](int t) { return *reinterpret_cast<const float *>(f.buf + t * f.stride + data_bytes); };
     if constexpr (TRAV == kTravF16) {
-        const int ks = (int)(row_bytes / 32);
+        const int ks = (int)(data_bytes / 32);
         const uint32_t *qw = reinterpret_cast<const uint32_t *>(qbuf);
         for (int t0 = 0; t0 < n; t0 += 16) {
             const int r = min(t0 + (lane & 15), n - 1);
@@ -226,8 +225,8 @@ __device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery
             // column 0: lanes 4g hold rows t0 + g (c0) and t0 + g + 8 (c2)
             if ((lane & 3) == 0) {
                 const int ra = t0 + (lane >> 2), rb = ra + 8;
-                if (ra < n) cd[ra] = ip ? -c0 : qnorm + cd[ra] - 2.f * c0;
-                if (rb < n) cd[rb] = ip ? -c2 : qnorm + cd[rb] - 2.f * c2;
+                if (ra < n) cd[ra] = ip ? -c0 : qnorm + xnorm(ra) - 2.f * c0;
+                if (rb < n) cd[rb] = ip ? -c2 : qnorm + xnorm(rb) - 2.f * c2;
             }
         }
     } else {
@@ -244,7 +243,7 @@ __device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery
                 }
             }
             for (int off = G >> 1; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off);
-            if (gl == 0 && t < n) cd[t] = ip ? -acc : qnorm - 2.f * acc + cd[t];
+            if (gl == 0 && t < n) cd[t] = ip ? -acc : qnorm - 2.f * acc + xnorm(t);
         }
     }
     __syncwarp();
@@ -466,9 +465,9 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
     uint8_t *qbuf = my + lay.qbuf;
     RowFetch f{my + lay.rowbuf, lay.stride, bar, 0u};
 
-    const TravView tv{a.trav, a.trav_zero, a.trav_row_bytes, a.rownorm};
+    const TravView tv{a.trav, a.trav_zero, a.trav_row_bytes};
     const bool ip = gp->metric == PK_METRIC_IP;
-    float *const norm_out = ip ? nullptr : cd;
+    const int64_t tdb = a.trav_data_bytes;
     const int enter_level = gp->enter_level;
     const int rb = a.rb;
     const int expand = max(1, min(a.expand, 4));
@@ -523,17 +522,17 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                 return r < a.trav_rows ? r : -1;
             };
             if (lane == 0) crow[0] = vrow(enter);
-            if (!fetch_rows(f, tv, crow, 1, norm_out, lane)) {
+            if (!fetch_rows(f, tv, crow, 1, lane)) {
                 failed = true;
                 break;
             }
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, 1, lane);
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, 1, lane);
             float best = cd[0];
             int32_t c = enter;
             bool moved = false;
             auto flush_up = [&](int nn) -> bool {
-                if (!fetch_rows(f, tv, crow, nn, norm_out, lane)) return false;
-                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, nn, lane);
+                if (!fetch_rows(f, tv, crow, nn, lane)) return false;
+                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, nn, lane);
                 float bd;
                 int bt;
                 warp_argmin(cd, nn, bd, bt, lane);
@@ -580,10 +579,10 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             __syncwarp();
             if (enter < 0 || enter >= lim0) enter = 0;
             if (lane == 0) crow[0] = enter;
-            if (!fetch_rows(f, tv, crow, 1, norm_out, lane)) failed = true;
+            if (!fetch_rows(f, tv, crow, 1, lane)) failed = true;
         }
         if (!failed) {
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, 1, lane);
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, 1, lane);
             const float d0 = cd[0];
             if (lane == 0) {
                 list.d[0] = d0;
@@ -594,8 +593,8 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             list.at(wl, wsl, wd, wi, lane);
         }
         auto flush0 = [&](int nn) -> bool {
-            if (!fetch_rows(f, tv, crow, nn, norm_out, lane)) return false;
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tv.row_bytes, qbuf, cd, nn, lane);
+            if (!fetch_rows(f, tv, crow, nn, lane)) return false;
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, nn, lane);
             cnt[4] += nn;
             for (int i0 = 0; i0 < nn; i0 += 32) {
                 const int i = i0 + lane;
@@ -853,10 +852,12 @@ __device__ __forceinline__ float elem(const uint8_t *row, int d) {
 }
 
 // Rows [r0, r1) of vec0 into the traversal copy (divided by the scales) and
-// the per-row sum of squares of the stored values.  One block per row.
+// the per-row sum of squares of the stored values (into rownorm and, with
+// norm_off >= 0, into the row at that byte).  One block per row.
 template <int DT, int TRAV>
 __global__ void convert_rows_kernel(const uint8_t *vec0, int64_t row_bytes, int64_t r0, int64_t r1, int dim,
-                                    const float *scale, uint8_t *trav, int64_t trav_row_bytes, float *rownorm) {
+                                    const float *scale, uint8_t *trav, int64_t trav_row_bytes, int64_t norm_off,
+                                    float *rownorm) {
     __shared__ float red[32];
     for (int64_t r = r0 + blockIdx.x; r < r1; r += gridDim.x) {
         const uint8_t *row = vec0 + r * row_bytes;
@@ -883,6 +884,7 @@ __global__ void convert_rows_kernel(const uint8_t *vec0, int64_t row_bytes, int6
             float sum = 0.f;
             for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += red[w];
             rownorm[r] = sum;
+            if (norm_off >= 0) *reinterpret_cast<float *>(out + norm_off) = sum;
         }
         __syncthreads();
     }
@@ -1011,23 +1013,23 @@ cudaError_t launch_absmax(int dtype, const uint8_t *vec0, int64_t row_bytes, int
 
 template <int DT>
 static void conv(int trav, const uint8_t *vec0, int64_t rb, int64_t r0, int64_t r1, int dim, const float *scale,
-                 uint8_t *t, int64_t trb, float *rn, cudaStream_t s) {
+                 uint8_t *t, int64_t trb, int64_t noff, float *rn, cudaStream_t s) {
     const int grid = (int)std::min<int64_t>(std::max<int64_t>(r1 - r0, 1), 8192);
     if (trav == kTravF16)
-        convert_rows_kernel<DT, kTravF16><<<grid, 128, 0, s>>>(vec0, rb, r0, r1, dim, scale, t, trb, rn);
+        convert_rows_kernel<DT, kTravF16><<<grid, 128, 0, s>>>(vec0, rb, r0, r1, dim, scale, t, trb, noff, rn);
     else
-        convert_rows_kernel<DT, kTravE4M3><<<grid, 128, 0, s>>>(vec0, rb, r0, r1, dim, scale, t, trb, rn);
+        convert_rows_kernel<DT, kTravE4M3><<<grid, 128, 0, s>>>(vec0, rb, r0, r1, dim, scale, t, trb, noff, rn);
 }
 
 cudaError_t launch_convert_rows(int dtype, int trav, const uint8_t *vec0, int64_t row_bytes, int64_t r0, int64_t r1,
                                 int dim, const float *scale, uint8_t *trav_rows, int64_t trav_row_bytes,
-                                float *rownorm, cudaStream_t s) {
+                                int64_t norm_off, float *rownorm, cudaStream_t s) {
     if (r1 <= r0) return cudaSuccess;
     switch (dtype) {
-        case PK_DTYPE_U8: conv<PK_DTYPE_U8>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, rownorm, s); break;
-        case PK_DTYPE_I8: conv<PK_DTYPE_I8>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, rownorm, s); break;
-        case PK_DTYPE_F32: conv<PK_DTYPE_F32>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, rownorm, s); break;
-        case PK_DTYPE_F16: conv<PK_DTYPE_F16>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, rownorm, s); break;
+        case PK_DTYPE_U8: conv<PK_DTYPE_U8>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, norm_off, rownorm, s); break;
+        case PK_DTYPE_I8: conv<PK_DTYPE_I8>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, norm_off, rownorm, s); break;
+        case PK_DTYPE_F32: conv<PK_DTYPE_F32>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, norm_off, rownorm, s); break;
+        case PK_DTYPE_F16: conv<PK_DTYPE_F16>(trav, vec0, row_bytes, r0, r1, dim, scale, trav_rows, trav_row_bytes, norm_off, rownorm, s); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -39,7 +39,7 @@ struct WalkArgs {
     const uint8_t *trav_zero;   // a zero row of the traversal copy
     int64_t trav_row_bytes;
     int64_t trav_rows;          // rows in the traversal copy; node ids stay below it
-    const float *rownorm;       // sum of squares of each stored row (L2)
+    int64_t trav_data_bytes;    // the values of a row; for L2 the row's norm follows them (float)
 };
 
 // Shared-memory stride of a staged traversal row: the row padded to an odd
@@ -133,9 +133,12 @@ cudaError_t launch_rerank(const DevGraph *g, int dtype, const LaneCfg &lc, const
                           size_t smem, cudaStream_t s);
 cudaError_t launch_absmax(int dtype, const uint8_t *vec0, int64_t row_bytes, int64_t n, int dim, uint32_t *out,
                           cudaStream_t s);
+// Rows [r0, r1) into the traversal copy; each row's sum of squares of the
+// stored values goes to rownorm[r] and, when norm_off >= 0, into the row at
+// byte norm_off.
 cudaError_t launch_convert_rows(int dtype, int trav, const uint8_t *vec0, int64_t row_bytes, int64_t r0, int64_t r1,
                                 int dim, const float *scale, uint8_t *trav_rows, int64_t trav_row_bytes,
-                                float *rownorm, cudaStream_t s);
+                                int64_t norm_off, float *rownorm, cudaStream_t s);
 cudaError_t launch_prep_queries(int dtype, int trav, const uint8_t *q, int64_t row_bytes, int64_t nq, int dim,
                                 const float *scale, uint8_t *out, int64_t out_row_bytes, float *qnorm,
                                 cudaStream_t s);

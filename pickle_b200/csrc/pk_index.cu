@@ -165,6 +165,7 @@ struct pk_index {
     // low-precision traversal copy and the fast path's scratch
     int trav = 0;                  // 0 none, pk::kTravF16, pk::kTravE4M3
     int64_t trav_row_bytes = 0, trav_rows = 0, trav_cap = 0;
+    int64_t trav_data_bytes = 0;   // the traversal values; L2 rows add a 16-byte chunk with the row's norm
     uint8_t *d_trav = nullptr, *d_trav_zero = nullptr;
     float *d_scale = nullptr, *d_rownorm = nullptr;
     float trav_f16_scale = 1.0f;   // FP16 copy = vectors / this power of two
@@ -748,8 +749,11 @@ float f16_scale(const std::vector<float> &m) {
 int build_traversal(pk_index *h, int trav) {
     cudaStream_t s = h->stream;
     // FP16 rows are padded with zeros to whole 16-element steps of the
-    // tensor-core dot products (32 bytes)
-    const int64_t trb = trav == pk::kTravF16 ? (h->dim * 2 + 31) / 32 * 32 : pk::align16(h->dim);
+    // tensor-core dot products (32 bytes); for L2 a 16-byte chunk after the
+    // values holds the row's sum of squares, so a row's bulk copy brings its
+    // norm along
+    const int64_t tdb = trav == pk::kTravF16 ? (h->dim * 2 + 31) / 32 * 32 : pk::align16(h->dim);
+    const int64_t trb = tdb + (h->metric == PK_METRIC_L2 ? 16 : 0);
     const int64_t rows = std::max<int64_t>(h->vec_rows, 1);
     PK_CUDA(cudaStreamSynchronize(s));
     dfree(h, h->d_trav, (size_t)(h->trav_cap * h->trav_row_bytes));
@@ -778,10 +782,11 @@ int build_traversal(pk_index *h, int trav) {
     }
     PK_CUDA(cudaMemcpyAsync(h->d_scale, scale.data(), 4 * (size_t)h->dim, cudaMemcpyHostToDevice, s));
     PK_CUDA(pk::launch_convert_rows(h->dtype, trav, h->hg.vec0, h->row_bytes, 0, h->n0(), (int)h->dim, h->d_scale,
-                                    h->d_trav, trb, h->d_rownorm, s));
+                                    h->d_trav, trb, h->metric == PK_METRIC_L2 ? tdb : -1, h->d_rownorm, s));
     PK_CUDA(cudaStreamSynchronize(s));
     h->trav = trav;
     h->trav_row_bytes = trb;
+    h->trav_data_bytes = tdb;
     h->trav_rows = h->n0();
     h->trav_cap = rows;
     return PK_OK;
@@ -801,7 +806,8 @@ int refresh_traversal(pk_index *h) {
         if (!(mx <= 32.0f * h->trav_f16_scale)) return build_traversal(h, h->trav);
     }
     PK_CUDA(pk::launch_convert_rows(h->dtype, h->trav, h->hg.vec0, h->row_bytes, h->trav_rows, h->n0(), (int)h->dim,
-                                    h->d_scale, h->d_trav, h->trav_row_bytes, h->d_rownorm, h->stream));
+                                    h->d_scale, h->d_trav, h->trav_row_bytes,
+                                    h->metric == PK_METRIC_L2 ? h->trav_data_bytes : -1, h->d_rownorm, h->stream));
     PK_CUDA(cudaStreamSynchronize(h->stream));
     h->trav_rows = h->n0();
     return PK_OK;
@@ -847,7 +853,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     const bool binned = ef_arr != nullptr && slots > 1;
     WalkShape ws;
     PK_TRY(walk_shape(h, ws));
-    const pk::TravCfgHost tc = pk::trav_config(h->trav_row_bytes, h->trav);
+    const pk::TravCfgHost tc = pk::trav_config(h->trav_data_bytes, h->trav);
     PK_TRY(ensure_buf(h, &c.d_work, c.work_n, kWorkInts));
     PK_TRY(ensure_buf(h, &c.d_cand, c.cand_n, nq * cs));
     if (binned) PK_TRY(ensure_buf(h, &c.d_lists, c.lists_n, nq * pk::kSlotClasses));
@@ -861,7 +867,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
                                   host_queries ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
         qx = c.d_fq;
     }
-    const int64_t tq_rb = h->trav == pk::kTravF16 ? h->trav_row_bytes : (h->trav_row_bytes / 16) * 64;
+    const int64_t tq_rb = h->trav == pk::kTravF16 ? h->trav_data_bytes : (h->trav_data_bytes / 16) * 64;
     PK_TRY(ensure_buf(h, &c.d_tq, c.tq_n, nq * tq_rb));
     PK_TRY(ensure_buf(h, &c.d_qn, c.qn_n, nq));
     PK_CUDA(pk::launch_prep_queries(h->dtype, h->trav, qx, h->row_bytes, nq, (int)h->dim, h->d_scale, c.d_tq, tq_rb,
@@ -887,8 +893,8 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     a.trav = h->d_trav;
     a.trav_zero = h->d_trav_zero;
     a.trav_row_bytes = h->trav_row_bytes;
+    a.trav_data_bytes = h->trav_data_bytes;
     a.trav_rows = h->trav_rows;
-    a.rownorm = h->d_rownorm;
     const bool timed = h->fast_timing && &c == &h->fctx;
     if (timed) {
         for (cudaEvent_t &e : c.ev)
