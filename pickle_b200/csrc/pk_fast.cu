@@ -775,7 +775,7 @@ __global__ void bin_by_slots_kernel(const int32_t *ef_arr, int32_t ef_bound, int
                                     int32_t *lists) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (int64_t)gridDim.x * blockDim.x) {
         const int ef = max(1, min(ef_arr[q], ef_bound));
-        const int c = __ffs(list_slots(ef)) - 1;
+        const int c = slot_class(ef);
         const int pos = atomicAdd(counts + c, 1);
         lists[(int64_t)c * nq + pos] = (int32_t)q;
     }
@@ -787,8 +787,11 @@ void *walk_pick_s(int s) {
     switch (s) {
         case 1: return (void *)walk_kernel<TRAV, KT, 1>;
         case 2: return (void *)walk_kernel<TRAV, KT, 2>;
+        case 3: return (void *)walk_kernel<TRAV, KT, 3>;
         case 4: return (void *)walk_kernel<TRAV, KT, 4>;
+        case 6: return (void *)walk_kernel<TRAV, KT, 6>;
         case 8: return (void *)walk_kernel<TRAV, KT, 8>;
+        case 12: return (void *)walk_kernel<TRAV, KT, 12>;
         case 16: return (void *)walk_kernel<TRAV, KT, 16>;
         default: return nullptr;
     }

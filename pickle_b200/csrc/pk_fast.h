@@ -99,31 +99,45 @@ struct RerankArgs {
     int64_t row_bytes;
 };
 
-// Shared memory of one re-rank warp: a Stage block, the sort buffers
-// (cand_stride distances and ids), kStageRows exact rows.
+__host__ __device__ inline int pow2_at_least(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// Shared memory of one re-rank warp: a Stage block, the sort buffers (the
+// bitonic sort pads a list to a power of two, so pow2_at_least(cand_stride)
+// distances and ids), kStageRows exact rows.
 struct RerankLayout {
     int sd, sid, rowbuf, total;
 };
 __host__ __device__ inline RerankLayout rerank_layout(int cand_stride, int64_t row_bytes) {
     RerankLayout r;
+    const int64_t sort_cap = pow2_at_least(cand_stride);
     r.sd = kStageBytes;
-    r.sid = r.sd + align16(4 * (int64_t)cand_stride);
-    r.rowbuf = r.sid + align16(4 * (int64_t)cand_stride);
+    r.sid = r.sd + align16(4 * sort_cap);
+    r.rowbuf = r.sid + align16(4 * sort_cap);
     r.total = align16(r.rowbuf + kStageRows * row_bytes);
     return r;
 }
 
-// List slots per lane (1, 2, 4, 8, 16) for an ef: the register list holds 32 per slot.
-__host__ __device__ inline int list_slots(int ef) {
-    int s = 1;
-    while (32 * s < ef && s < kFastMaxEf / 32) s *= 2;
-    return s;
+// List widths: slots per lane of the register list, which holds 32 entries
+// per slot.  A query takes the narrowest width that holds its ef, so its list
+// is at most a third wider than ef.
+constexpr int kSlotClasses = 8;
+__host__ __device__ inline int slot_class_width(int c) {
+    return c < 3 ? c + 1 : c == 3 ? 4 : c == 4 ? 6 : c == 5 ? 8 : c == 6 ? 12 : 16;  // 1 2 3 4 6 8 12 16
 }
-constexpr int kSlotClasses = 5;  // slots 1, 2, 4, 8, 16
+__host__ __device__ inline int slot_class(int ef) {
+    int c = 0;
+    while (c < kSlotClasses - 1 && 32 * slot_class_width(c) < ef) c++;
+    return c;
+}
+__host__ __device__ inline int list_slots(int ef) { return slot_class_width(slot_class(ef)); }
 
 int walk_blocks_per_sm(int trav, const TravCfgHost &tc, int slots, int wpb, size_t smem);
-// Sorts the queries by list slots: lists[c * nq + i] = the i-th query with
-// 2^c slots, counts[c] = how many (counts zeroed by the caller).
+// Sorts the queries by list width class: lists[c * nq + i] = the i-th query
+// of class c, counts[c] = how many (counts zeroed by the caller).
 cudaError_t launch_bin_by_slots(const int32_t *ef_arr, int32_t ef_bound, int64_t nq, int32_t *counts,
                                 int32_t *lists, cudaStream_t s);
 cudaError_t launch_walk(const DevGraph *g, int trav, const TravCfgHost &tc, int slots, const WalkArgs &a, int grid,

@@ -901,8 +901,8 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
             if (!e) PK_CUDA(cudaEventCreate(&e));
         PK_CUDA(cudaEventRecord(c.ev[0], s));
     }
-    for (int cls = 0; (1 << cls) <= slots; cls++) {
-        const int sl = 1 << cls;
+    for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
+        const int sl = pk::slot_class_width(cls);
         if (!binned && sl != slots) continue;
         const int nb = pk::walk_blocks_per_sm(h->trav, tc, sl, ws.wpb, ws.smem);
         if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");

@@ -122,9 +122,9 @@ def test_fast_launch_shapes_keep_results(shape, expand, gpu, ref_bin):
     assert r_exp >= r_one - 0.01, (r_exp, r_one)
 
 
-@pytest.mark.parametrize("ef", [1, 10, 33, 64, 65, 257, 512])
+@pytest.mark.parametrize("ef", [1, 10, 33, 64, 65, 97, 193, 257, 385, 512])
 def test_fast_list_sizes(ef, gpu, ref_bin):
-    """Every list width (1..16 slots per lane), k up to ef."""
+    """Every list width (1, 2, 3, 4, 6, 8, 12, 16 slots per lane), k up to ef."""
     metric, base, queries, M, efc = case_data("f32unit_ip")
     idx = HNSWIndex.load(ref_graph("f32unit_ip"))
     idx.prepare_fast("f16")
