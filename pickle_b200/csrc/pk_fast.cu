@@ -58,38 +58,18 @@ struct TravCfg {
     int GT, KT, CT;
 };
 
-// FP16 traversal: rows and queries are stored divided by one power of two
-// that brings the largest stored magnitude into [4, 8) (a power of two
-// changes no rounding and no order of distances).  Dot products run on the
-// tensor cores (trav_dist_buf); the query is staged in shared memory.
-// E4M3 traversal: the query is held as 16 floats per chunk (pre-scaled).
+// Traversal formats; both walk with tensor-core dot products (trav_dist_buf)
+// and stage the query in shared memory.
+// FP16: rows and queries are stored divided by one power of two that brings
+// the largest stored magnitude into [4, 8) (a power of two changes no
+// rounding and no order of distances).
+// FP8 E4M3: rows are stored divided by per-dimension scales (largest
+// magnitude onto 448); a query is multiplied by the same scales, brought into
+// E4M3's range by a power of two, and stored as two E4M3 parts - its rounding
+// and the rounding of the remainder - so that two products recover it to
+// about 0.02% per component; the power of two is undone after the product.
 template <int TRAV, int KT>
-struct TravQuery;
-
-template <int KT>
-struct TravQuery<kTravF16, KT> {};
-
-template <int KT>
-struct TravQuery<kTravE4M3, KT> {
-    float q[KT][16];
-    __device__ __forceinline__ float dot(const uint4 &r, int k) const {
-        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
-        float a = 0.f;
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const __nv_fp8x2_storage_t lo = (__nv_fp8x2_storage_t)(w[i] & 0xffffu);
-            const __nv_fp8x2_storage_t hi = (__nv_fp8x2_storage_t)(w[i] >> 16);
-            const __half2 h0 = __half2(__nv_cvt_fp8x2_to_halfraw2(lo, __NV_E4M3));
-            const __half2 h1 = __half2(__nv_cvt_fp8x2_to_halfraw2(hi, __NV_E4M3));
-            const float2 f0 = __half22float2(h0), f1 = __half22float2(h1);
-            a = fmaf(q[k][4 * i + 0], f0.x, a);
-            a = fmaf(q[k][4 * i + 1], f0.y, a);
-            a = fmaf(q[k][4 * i + 2], f1.x, a);
-            a = fmaf(q[k][4 * i + 3], f1.y, a);
-        }
-        return a;
-    }
-};
+struct TravQuery {};
 
 struct TravView {
     const uint8_t *rows;      // traversal copy, row_bytes apart
@@ -182,68 +162,74 @@ __device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, cons
     return all;
 }
 
+// One tensor-core step: the 16 staged rows' fragment a times the query's
+// fragment (b0, b1), accumulated into c.  FP16: k = 16 elements; E4M3: k = 32.
+template <int TRAV>
+__device__ __forceinline__ void mma_step(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    if constexpr (TRAV == kTravF16)
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+            "{%0, %1, %2, %3};"
+            : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    else
+        asm volatile(
+            "mma.sync.aligned.m16n8k32.row.col.f32.e4m3.e4m3.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+            "{%0, %1, %2, %3};"
+            : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
 // Traversal distances of the n staged rows to the query, into cd[t].  A row's
-// values take data_bytes; for L2 its stored norm (float) follows them.  All
-// lanes call.
+// values take data_bytes (whole 32-byte steps); for L2 its stored norm
+// (float) follows them.  All lanes call.
 //
-// FP16: the tensor cores.  Sixteen staged rows at a time are the A operand of
-// mma.m16n8k16 (ldmatrix takes one row address per lane, so the gathered rows
-// need no particular layout), the query is column 0 of B (lanes 0-3 hold its
-// fragment; B's other columns are zero), and column 0 of the FP32
-// accumulator holds the 16 dot products.  L2 = |q|^2 + |x|^2 - 2 q.x from
-// the stored norms of the same FP16 values.
-// E4M3: groups of G lanes per row, FP32 FMAs over the decoded elements.
+// Sixteen staged rows at a time are the A operand of mma.m16n8k16 (FP16) or
+// mma.m16n8k32 (E4M3): ldmatrix takes one row address per lane, so gathered
+// rows need no particular layout, and a 32-byte step of a row is one k-step
+// in both formats.  The query is column 0 of B (lanes 0-3 hold its fragment;
+// B's other columns are zero), and column 0 of the FP32 accumulator holds the
+// 16 dot products.  E4M3 multiplies by the query's two parts (the second
+// starts data_bytes into the staged query) and scales the sum by qfac.
+// L2 = |q|^2 + |x|^2 - 2 q.x from the stored norms of the same values.
 template <int TRAV, int KT>
-__device__ __forceinline__ void trav_dist_buf(const TravCfg &tc, const TravQuery<TRAV, KT> &tq, bool ip, float qnorm,
-                                              const RowFetch &f, int64_t data_bytes, const uint8_t *qbuf, float *cd,
-                                              int n, int lane) {
+__device__ __forceinline__ void trav_dist_buf(const TravCfg &, const TravQuery<TRAV, KT> &, bool ip, float qnorm,
+                                              float qfac, const RowFetch &f, int64_t data_bytes, const uint8_t *qbuf,
+                                              float *cd, int n, int lane) {
     auto xnorm = [&](int t) { return *reinterpret_cast<const float *>(f.buf + t * f.stride + data_bytes); };
-    if constexpr (TRAV == kTravF16) {
-        const int ks = (int)(data_bytes / 32);
-        const uint32_t *qw = reinterpret_cast<const uint32_t *>(qbuf);
-        for (int t0 = 0; t0 < n; t0 += 16) {
-            const int r = min(t0 + (lane & 15), n - 1);
-            const uint32_t arow = smem_u32(f.buf + r * f.stride) + (uint32_t)(lane >> 4) * 16u;
-            float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
-            for (int kk = 0; kk < ks; kk++) {
-                uint32_t a0, a1, a2, a3;
-                asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
-                             : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
-                             : "r"(arow + (uint32_t)kk * 32u)
-                             : "memory");
-                uint32_t b0 = 0, b1 = 0;
-                if (lane < 4) {
-                    b0 = qw[kk * 8 + lane];
-                    b1 = qw[kk * 8 + 4 + lane];
-                }
-                asm volatile(
-                    "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-                    "{%0, %1, %2, %3};"
-                    : "+f"(c0), "+f"(c1), "+f"(c2), "+f"(c3)
-                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    const int ks = (int)(data_bytes / 32);
+    const uint32_t *qw = reinterpret_cast<const uint32_t *>(qbuf);
+    const int low = (int)(data_bytes / 4);  // E4M3: first word of the query's second part
+    for (int t0 = 0; t0 < n; t0 += 16) {
+        const int r = min(t0 + (lane & 15), n - 1);
+        const uint32_t arow = smem_u32(f.buf + r * f.stride) + (uint32_t)(lane >> 4) * 16u;
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kk = 0; kk < ks; kk++) {
+            uint32_t a[4];
+            asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+                         : "r"(arow + (uint32_t)kk * 32u)
+                         : "memory");
+            uint32_t b0 = 0, b1 = 0;
+            if (lane < 4) {
+                b0 = qw[kk * 8 + lane];
+                b1 = qw[kk * 8 + 4 + lane];
             }
-            // column 0: lanes 4g hold rows t0 + g (c0) and t0 + g + 8 (c2)
-            if ((lane & 3) == 0) {
-                const int ra = t0 + (lane >> 2), rb = ra + 8;
-                if (ra < n) cd[ra] = ip ? -c0 : qnorm + xnorm(ra) - 2.f * c0;
-                if (rb < n) cd[rb] = ip ? -c2 : qnorm + xnorm(rb) - 2.f * c2;
+            mma_step<TRAV>(c, a, b0, b1);
+            if constexpr (TRAV == kTravE4M3) {
+                if (lane < 4) {
+                    b0 = qw[low + kk * 8 + lane];
+                    b1 = qw[low + kk * 8 + 4 + lane];
+                }
+                mma_step<TRAV>(c, a, b0, b1);
             }
         }
-    } else {
-        const int G = tc.GT, R = 32 / G, grp = lane / G, gl = lane % G;
-        for (int base = 0; base < n; base += R) {
-            const int t = base + grp;
-            float acc = 0.f;
-            if (t < n) {
-                const uint8_t *row = f.buf + t * f.stride;
-#pragma unroll
-                for (int k = 0; k < KT; k++) {
-                    const int c = gl + k * G;
-                    if (c < tc.CT) acc += tq.dot(*reinterpret_cast<const uint4 *>(row + c * 16), k);
-                }
-            }
-            for (int off = G >> 1; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off);
-            if (gl == 0 && t < n) cd[t] = ip ? -acc : qnorm - 2.f * acc + xnorm(t);
+        // column 0: lanes 4g hold rows t0 + g (c[0]) and t0 + g + 8 (c[2])
+        if ((lane & 3) == 0) {
+            const int ra = t0 + (lane >> 2), rb = ra + 8;
+            const float da = c[0] * qfac, db = c[2] * qfac;
+            if (ra < n) cd[ra] = ip ? -da : qnorm + xnorm(ra) - 2.f * da;
+            if (rb < n) cd[rb] = ip ? -db : qnorm + xnorm(rb) - 2.f * db;
         }
     }
     __syncwarp();
@@ -438,16 +424,16 @@ __device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, i
 }
 
 // ------------------------------------------------------------------ walk ---
-// Narrow lists (ef <= 128) fit 80 registers per thread without spills, so
-// three 256-thread blocks can be resident per SM; wider lists, and E4M3
-// queries of more than one chunk per lane, take two.
+// Narrow FP16 lists (ef <= 128) fit 80 registers per thread without spills,
+// so three 256-thread blocks can be resident per SM; wider lists and the E4M3
+// walk (two query parts per k-step) take two.
 template <int TRAV, int KT, int S>
-__global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1)) ? 3 : 2)
+__global__ void __launch_bounds__(256, (S <= 4 && TRAV == kTravF16) ? 3 : 2)
     walk_kernel(const DevGraph *__restrict__ gp, const TravCfg tc, const WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const WalkLayout lay = walk_layout(a.rb, a.trav_row_bytes, a.hlog2, a.tag16 != 0);
+    const WalkLayout lay = walk_layout(a.rb, a.trav_row_bytes, a.tq_row_bytes, a.hlog2, a.tag16 != 0);
     unsigned char *my = smem + (size_t)wib * lay.total;
     SeenTable seen;
     seen.w = reinterpret_cast<uint32_t *>(my + lay.tab);
@@ -484,30 +470,16 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
         const int64_t q = a.qlist ? a.qlist[qi] : qi;
         const int L = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, 32 * S));
 
-        // the query in the traversal format: FP16 staged in shared memory,
-        // E4M3 as this lane's chunks in registers
+        // the query in the traversal format, staged in shared memory
         TravQuery<TRAV, KT> tq;
         const float qnorm = ip ? 0.f : a.qnorm[q];
+        float qfac = 1.f;
         {
             const uint8_t *qrow = a.tq_rows + q * a.tq_row_bytes;
-            if constexpr (TRAV == kTravF16) {
-                for (int c = lane; c < (int)(a.tq_row_bytes / 16); c += 32)
-                    reinterpret_cast<uint4 *>(qbuf)[c] = ld16(qrow + c * 16);
-                __syncwarp();
-            } else {
-                const int G = tc.GT, gl = lane % G;
-#pragma unroll
-                for (int kk = 0; kk < KT; kk++) {
-                    const int c = gl + kk * G;
-#pragma unroll
-                    for (int e = 0; e < 16; e++) tq.q[kk][e] = 0.f;
-                    if (c < tc.CT) {
-                        const float *qf = reinterpret_cast<const float *>(qrow) + c * 16;
-#pragma unroll
-                        for (int e = 0; e < 16; e++) tq.q[kk][e] = qf[e];
-                    }
-                }
-            }
+            for (int c = lane; c < (int)(a.tq_row_bytes / 16); c += 32)
+                reinterpret_cast<uint4 *>(qbuf)[c] = ld16(qrow + c * 16);
+            __syncwarp();
+            if (TRAV == kTravE4M3) qfac = *reinterpret_cast<const float *>(qbuf + 2 * a.trav_data_bytes);
         }
 
         int32_t cnt[6] = {0, 0, 0, 0, 0, 0};
@@ -526,13 +498,13 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
                 failed = true;
                 break;
             }
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, 1, lane);
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
             float best = cd[0];
             int32_t c = enter;
             bool moved = false;
             auto flush_up = [&](int nn) -> bool {
                 if (!fetch_rows(f, tv, crow, nn, lane)) return false;
-                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, nn, lane);
+                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, nn, lane);
                 float bd;
                 int bt;
                 warp_argmin(cd, nn, bd, bt, lane);
@@ -582,7 +554,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
             if (!fetch_rows(f, tv, crow, 1, lane)) failed = true;
         }
         if (!failed) {
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, 1, lane);
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
             const float d0 = cd[0];
             if (lane == 0) {
                 list.d[0] = d0;
@@ -594,7 +566,7 @@ __global__ void __launch_bounds__(256, (S <= 4 && (TRAV == kTravF16 || KT == 1))
         }
         auto flush0 = [&](int nn) -> bool {
             if (!fetch_rows(f, tv, crow, nn, lane)) return false;
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, f, tdb, qbuf, cd, nn, lane);
+            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, nn, lane);
             cnt[4] += nn;
             for (int i0 = 0; i0 < nn; i0 += 32) {
                 const int i = i0 + lane;
@@ -798,13 +770,8 @@ void *walk_pick_s(int s) {
 }
 void *walk_kernel_ptr(int trav, int kt, int s) {
     if (trav == kTravF16) return kt == 1 ? walk_pick_s<kTravF16, 1>(s) : nullptr;
-    if (trav != kTravE4M3) return nullptr;
-    switch (kt) {
-        case 1: return walk_pick_s<kTravE4M3, 1>(s);
-        case 2: return walk_pick_s<kTravE4M3, 2>(s);
-        case 4: return walk_pick_s<kTravE4M3, 4>(s);
-        default: return nullptr;
-    }
+    if (trav == kTravE4M3) return kt == 1 ? walk_pick_s<kTravE4M3, 1>(s) : nullptr;
+    return nullptr;
 }
 
 template <int DT>
@@ -893,33 +860,61 @@ __global__ void convert_rows_kernel(const uint8_t *vec0, int64_t row_bytes, int6
     }
 }
 
-// Queries into the traversal format.  FP16: rows of halves divided by the
-// scale (clamped to 64 scaled units: the copy's rows stay within 32), zero
-// padded, plus the sum of squares of the stored halves.  E4M3: rows of floats
-// pre-multiplied by the per-dimension scales (padded to a multiple of 16
-// elements) plus sum_d q_d^2.
+// Queries into the traversal format (rows of out_row_bytes; data_bytes of
+// values) and their sums of squares.  FP16: halves divided by the scale
+// (clamped to 64 scaled units: the copy's rows stay within 32), zero padded;
+// qnorm = sum of the stored halves' squares.  E4M3: q_d * scale_d times a
+// power of two p bringing the largest magnitude into [128, 256), stored as
+// its E4M3 rounding (bytes [0, data_bytes)) and the E4M3 rounding of the
+// remainder (bytes [data_bytes, 2 data_bytes)), then the float 1/p; qnorm =
+// sum of q_d^2.
 template <int DT, int TRAV>
 __global__ void prep_queries_kernel(const uint8_t *q, int64_t row_bytes, int64_t nq, int dim, const float *scale,
-                                    uint8_t *out, int64_t out_row_bytes, float *qnorm) {
+                                    uint8_t *out, int64_t out_row_bytes, int64_t data_bytes, float *qnorm) {
     __shared__ float red[32];
+    __shared__ float pmul;
     for (int64_t r = blockIdx.x; r < nq; r += gridDim.x) {
         const uint8_t *row = q + r * row_bytes;
         uint8_t *o = out + r * out_row_bytes;
         float part = 0.f;
-        const int padded = TRAV == kTravF16 ? (int)(out_row_bytes / 2) : (int)(out_row_bytes / 4);
-        for (int d = threadIdx.x; d < padded; d += blockDim.x) {
-            const float v = d < dim ? elem<DT>(row, d) : 0.f;
-            if constexpr (TRAV == kTravF16) {
+        if constexpr (TRAV == kTravF16) {
+            const int padded = (int)(data_bytes / 2);
+            for (int d = threadIdx.x; d < padded; d += blockDim.x) {
+                const float v = d < dim ? elem<DT>(row, d) : 0.f;
                 const __half h = __float2half_rn(d < dim ? fminf(fmaxf(v / scale[d], -64.f), 64.f) : 0.f);
                 reinterpret_cast<__half *>(o)[d] = h;
                 const float b = __half2float(h);
                 part += b * b;
-            } else {
-                reinterpret_cast<float *>(o)[d] = d < dim ? v * scale[d] : 0.f;
+            }
+        } else {
+            // largest |q_d * scale_d| of the query, then the power of two
+            float mx = 0.f;
+            for (int d = threadIdx.x; d < dim; d += blockDim.x) mx = fmaxf(mx, fabsf(elem<DT>(row, d) * scale[d]));
+            for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, off));
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                float m = 0.f;
+                for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, red[w]);
+                int e = 0;
+                if (m > 0.f && isfinite(m)) frexpf(m, &e);  // m = f * 2^e, f in [0.5, 1)
+                pmul = (m > 0.f && isfinite(m)) ? ldexpf(1.f, 8 - e) : 1.f;  // m * pmul in [128, 256)
+            }
+            __syncthreads();
+            const float pm = pmul;
+            for (int d = threadIdx.x; d < (int)data_bytes; d += blockDim.x) {
+                const float v = d < dim ? elem<DT>(row, d) : 0.f;
+                const float x = d < dim ? v * scale[d] * pm : 0.f;
+                const __nv_fp8_storage_t hi = __nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
+                const float back = __half2float(__half(__nv_cvt_fp8_to_halfraw(hi, __NV_E4M3)));
+                o[d] = hi;
+                o[data_bytes + d] = __nv_cvt_float_to_fp8(x - back, __NV_SATFINITE, __NV_E4M3);
                 part += v * v;
             }
+            if (threadIdx.x == 0) *reinterpret_cast<float *>(o + 2 * data_bytes) = 1.f / pm;
         }
         for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(kFull, part, off);
+        __syncthreads();
         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -933,25 +928,14 @@ __global__ void prep_queries_kernel(const uint8_t *q, int64_t row_bytes, int64_t
 
 }  // namespace
 
-TravCfgHost trav_config(int64_t trav_row_bytes, int trav) {
+TravCfgHost trav_config(int64_t trav_data_bytes, int trav) {
+    // both formats run on the tensor cores with the query in shared memory;
+    // one instantiation per list width
     TravCfgHost t;
-    t.CT = (int)(trav_row_bytes / 16);
-    if (trav == kTravF16) {
-        // the tensor-core path keeps the query in shared memory
-        t.GT = 32;
-        t.KT = 1;
-        t.KTMAX = 1;
-        return t;
-    }
-    // E4M3: a chunk holds 16 elements, whose query part is 16 floats, so a
-    // lane keeps one chunk; groups of G lanes (a power of two) per row
-    int G = 1;
-    while (G < t.CT && G < 32) G *= 2;
-    t.GT = G;
-    t.KT = (t.CT + G - 1) / G;
-    int kt = 1;
-    while (kt < t.KT) kt *= 2;
-    t.KTMAX = kt;
+    t.CT = (int)(trav_data_bytes / 16);
+    t.GT = 32;
+    t.KT = 1;
+    t.KTMAX = trav == kTravF16 || trav == kTravE4M3 ? 1 : 0;
     return t;
 }
 
@@ -1040,23 +1024,23 @@ cudaError_t launch_convert_rows(int dtype, int trav, const uint8_t *vec0, int64_
 
 template <int DT>
 static void prep(int trav, const uint8_t *q, int64_t rb, int64_t nq, int dim, const float *scale, uint8_t *out,
-                 int64_t orb, float *qn, cudaStream_t s) {
+                 int64_t orb, int64_t db, float *qn, cudaStream_t s) {
     const int grid = (int)std::min<int64_t>(std::max<int64_t>(nq, 1), 8192);
     if (trav == kTravF16)
-        prep_queries_kernel<DT, kTravF16><<<grid, 128, 0, s>>>(q, rb, nq, dim, scale, out, orb, qn);
+        prep_queries_kernel<DT, kTravF16><<<grid, 128, 0, s>>>(q, rb, nq, dim, scale, out, orb, db, qn);
     else
-        prep_queries_kernel<DT, kTravE4M3><<<grid, 128, 0, s>>>(q, rb, nq, dim, scale, out, orb, qn);
+        prep_queries_kernel<DT, kTravE4M3><<<grid, 128, 0, s>>>(q, rb, nq, dim, scale, out, orb, db, qn);
 }
 
 cudaError_t launch_prep_queries(int dtype, int trav, const uint8_t *q, int64_t row_bytes, int64_t nq, int dim,
-                                const float *scale, uint8_t *out, int64_t out_row_bytes, float *qnorm,
-                                cudaStream_t s) {
+                                const float *scale, uint8_t *out, int64_t out_row_bytes, int64_t data_bytes,
+                                float *qnorm, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
     switch (dtype) {
-        case PK_DTYPE_U8: prep<PK_DTYPE_U8>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, qnorm, s); break;
-        case PK_DTYPE_I8: prep<PK_DTYPE_I8>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, qnorm, s); break;
-        case PK_DTYPE_F32: prep<PK_DTYPE_F32>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, qnorm, s); break;
-        case PK_DTYPE_F16: prep<PK_DTYPE_F16>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, qnorm, s); break;
+        case PK_DTYPE_U8: prep<PK_DTYPE_U8>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, data_bytes, qnorm, s); break;
+        case PK_DTYPE_I8: prep<PK_DTYPE_I8>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, data_bytes, qnorm, s); break;
+        case PK_DTYPE_F32: prep<PK_DTYPE_F32>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, data_bytes, qnorm, s); break;
+        case PK_DTYPE_F16: prep<PK_DTYPE_F16>(trav, q, row_bytes, nq, dim, scale, out, out_row_bytes, data_bytes, qnorm, s); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

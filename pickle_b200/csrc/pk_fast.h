@@ -13,7 +13,13 @@ constexpr int kFastMaxEf = 512;  // the walk's register list holds up to 32 * 16
 struct TravCfgHost {
     int GT, KT, CT, KTMAX;
 };
-TravCfgHost trav_config(int64_t trav_row_bytes, int trav);
+TravCfgHost trav_config(int64_t trav_data_bytes, int trav);
+
+// Bytes of a traversal query row: FP16 = the values; E4M3 = the query's two
+// E4M3 parts and a 16-byte chunk holding its power-of-two factor.
+__host__ __device__ inline int64_t trav_query_bytes(int trav, int64_t trav_data_bytes) {
+    return trav == kTravF16 ? trav_data_bytes : 2 * trav_data_bytes + 16;
+}
 
 // Walk launch parameters.
 struct WalkArgs {
@@ -69,12 +75,13 @@ struct WalkLayout {
     int rowbuf, qbuf, tab, crow, cid, cd, bar, total;
     int64_t stride;
 };
-__host__ __device__ inline WalkLayout walk_layout(int rb, int64_t trav_row_bytes, int hlog2, bool tag16) {
+__host__ __device__ inline WalkLayout walk_layout(int rb, int64_t trav_row_bytes, int64_t query_bytes, int hlog2,
+                                                  bool tag16) {
     WalkLayout w;
     w.stride = stage_stride(trav_row_bytes);
     w.rowbuf = 0;
     w.qbuf = align16((int64_t)rb * w.stride);
-    w.tab = w.qbuf + align16(trav_row_bytes);
+    w.tab = w.qbuf + align16(query_bytes);
     w.crow = w.tab + ((tag16 ? 2 : 4) << hlog2);
     w.cid = w.crow + align16(4 * (int64_t)rb);
     w.cd = w.cid + align16(4 * (int64_t)rb);
@@ -154,7 +161,7 @@ cudaError_t launch_convert_rows(int dtype, int trav, const uint8_t *vec0, int64_
                                 int dim, const float *scale, uint8_t *trav_rows, int64_t trav_row_bytes,
                                 int64_t norm_off, float *rownorm, cudaStream_t s);
 cudaError_t launch_prep_queries(int dtype, int trav, const uint8_t *q, int64_t row_bytes, int64_t nq, int dim,
-                                const float *scale, uint8_t *out, int64_t out_row_bytes, float *qnorm,
-                                cudaStream_t s);
+                                const float *scale, uint8_t *out, int64_t out_row_bytes, int64_t data_bytes,
+                                float *qnorm, cudaStream_t s);
 
 }  // namespace pk

@@ -748,12 +748,12 @@ float f16_scale(const std::vector<float> &m) {
 // converted, with its stored norm.
 int build_traversal(pk_index *h, int trav) {
     cudaStream_t s = h->stream;
-    // FP16 rows are padded with zeros to whole 16-element steps of the
-    // tensor-core dot products (32 bytes); for L2 a 16-byte chunk after the
-    // values holds the row's sum of squares, so a row's bulk copy brings its
-    // norm along
-    const int64_t tdb = trav == pk::kTravF16 ? (h->dim * 2 + 31) / 32 * 32 : pk::align16(h->dim);
-    const int64_t trb = tdb + (h->metric == PK_METRIC_L2 ? 16 : 0);
+    // values padded with zeros to whole 32-byte steps of the tensor-core dot
+    // products (16 FP16 or 32 E4M3 elements); for L2 a 32-byte chunk after
+    // them holds the row's sum of squares, so a row's bulk copy brings its
+    // norm along and rows stay on whole 32-byte sectors
+    const int64_t tdb = trav == pk::kTravF16 ? (h->dim * 2 + 31) / 32 * 32 : (h->dim + 31) / 32 * 32;
+    const int64_t trb = tdb + (h->metric == PK_METRIC_L2 ? 32 : 0);
     const int64_t rows = std::max<int64_t>(h->vec_rows, 1);
     PK_CUDA(cudaStreamSynchronize(s));
     dfree(h, h->d_trav, (size_t)(h->trav_cap * h->trav_row_bytes));
@@ -829,10 +829,11 @@ int walk_shape(const pk_index *h, WalkShape &w) {
     const int64_t ids = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
     w.tag16 = pk::seen_tag16(ids, w.hlog2);
     w.idbits = std::max(pk::idbits_for(ids), w.hlog2 - 2);
-    w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2, w.tag16).total;
+    const int64_t qb = pk::trav_query_bytes(h->trav, h->trav_data_bytes);
+    w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, qb, w.hlog2, w.tag16).total;
     while (w.wpb > 1 && w.smem > 200 * 1024) {
         w.wpb /= 2;
-        w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, w.hlog2, w.tag16).total;
+        w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, qb, w.hlog2, w.tag16).total;
     }
     if (w.smem > 227 * 1024) return fail(PK_ERR_ARG, "walk working set exceeds shared memory: lower rows or filter bits");
     return PK_OK;
@@ -867,11 +868,11 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
                                   host_queries ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
         qx = c.d_fq;
     }
-    const int64_t tq_rb = h->trav == pk::kTravF16 ? h->trav_data_bytes : (h->trav_data_bytes / 16) * 64;
+    const int64_t tq_rb = pk::trav_query_bytes(h->trav, h->trav_data_bytes);
     PK_TRY(ensure_buf(h, &c.d_tq, c.tq_n, nq * tq_rb));
     PK_TRY(ensure_buf(h, &c.d_qn, c.qn_n, nq));
     PK_CUDA(pk::launch_prep_queries(h->dtype, h->trav, qx, h->row_bytes, nq, (int)h->dim, h->d_scale, c.d_tq, tq_rb,
-                                    c.d_qn, s));
+                                    h->trav_data_bytes, c.d_qn, s));
     PK_CUDA(cudaMemsetAsync(c.d_work, 0, sizeof(int32_t) * kWorkInts, s));
     if (binned) PK_CUDA(pk::launch_bin_by_slots(ef_arr, ef, nq, c.d_work + kWorkCounts, c.d_lists, s));
     pk::WalkArgs a{};
