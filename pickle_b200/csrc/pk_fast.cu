@@ -189,8 +189,9 @@ __device__ __forceinline__ void mma_step(float (&c)[4], const uint32_t (&a)[4], 
 // rows need no particular layout, and a 32-byte step of a row is one k-step
 // in both formats.  The query is column 0 of B (lanes 0-3 hold its fragment;
 // B's other columns are zero), and column 0 of the FP32 accumulator holds the
-// 16 dot products.  E4M3 multiplies by the query's two parts (the second
-// starts data_bytes into the staged query) and scales the sum by qfac.
+// 16 dot products.  E4M3 puts the query's second part (data_bytes into the
+// staged query) in column 1 (lanes 4-7), so one product per k-step yields
+// both; a row's dot product is columns 0 + 1, scaled by qfac.
 // L2 = |q|^2 + |x|^2 - 2 q.x from the stored norms of the same values.
 template <int TRAV, int KT>
 __device__ __forceinline__ void trav_dist_buf(const TravCfg &, const TravQuery<TRAV, KT> &, bool ip, float qnorm,
@@ -211,23 +212,19 @@ __device__ __forceinline__ void trav_dist_buf(const TravCfg &, const TravQuery<T
                          : "r"(arow + (uint32_t)kk * 32u)
                          : "memory");
             uint32_t b0 = 0, b1 = 0;
-            if (lane < 4) {
-                b0 = qw[kk * 8 + lane];
-                b1 = qw[kk * 8 + 4 + lane];
+            if (TRAV == kTravF16 ? lane < 4 : lane < 8) {
+                const int w = (TRAV == kTravE4M3 && lane >= 4 ? low : 0) + kk * 8 + (lane & 3);
+                b0 = qw[w];
+                b1 = qw[w + 4];
             }
             mma_step<TRAV>(c, a, b0, b1);
-            if constexpr (TRAV == kTravE4M3) {
-                if (lane < 4) {
-                    b0 = qw[low + kk * 8 + lane];
-                    b1 = qw[low + kk * 8 + 4 + lane];
-                }
-                mma_step<TRAV>(c, a, b0, b1);
-            }
         }
-        // column 0: lanes 4g hold rows t0 + g (c[0]) and t0 + g + 8 (c[2])
+        // columns 0 and 1: lane 4g holds row t0 + g in c[0], c[1] and row
+        // t0 + g + 8 in c[2], c[3]; column 1 is zero for FP16
         if ((lane & 3) == 0) {
             const int ra = t0 + (lane >> 2), rb = ra + 8;
-            const float da = c[0] * qfac, db = c[2] * qfac;
+            const float da = TRAV == kTravE4M3 ? (c[0] + c[1]) * qfac : c[0];
+            const float db = TRAV == kTravE4M3 ? (c[2] + c[3]) * qfac : c[2];
             if (ra < n) cd[ra] = ip ? -da : qnorm + xnorm(ra) - 2.f * da;
             if (rb < n) cd[rb] = ip ? -db : qnorm + xnorm(rb) - 2.f * db;
         }
@@ -424,11 +421,10 @@ __device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, i
 }
 
 // ------------------------------------------------------------------ walk ---
-// Narrow FP16 lists (ef <= 128) fit 80 registers per thread without spills,
-// so three 256-thread blocks can be resident per SM; wider lists and the E4M3
-// walk (two query parts per k-step) take two.
+// Narrow lists (ef <= 128) fit 80 registers per thread without spills, so
+// three 256-thread blocks can be resident per SM; wider lists take two.
 template <int TRAV, int KT, int S>
-__global__ void __launch_bounds__(256, (S <= 4 && TRAV == kTravF16) ? 3 : 2)
+__global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
     walk_kernel(const DevGraph *__restrict__ gp, const TravCfg tc, const WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
