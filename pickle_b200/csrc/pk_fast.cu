@@ -51,13 +51,6 @@ using namespace dev;
 constexpr uint32_t kExpanded = 0x80000000u;
 
 // ------------------------------------------------------- traversal distances
-// E4M3 lane layout: CT 16-byte chunks per row, GT lanes per row (power of
-// two >= CT, at most 32), KT chunks per lane.
-
-struct TravCfg {
-    int GT, KT, CT;
-};
-
 // Traversal formats; both walk with tensor-core dot products (trav_dist_buf)
 // and stage the query in shared memory.
 // FP16: rows and queries are stored divided by one power of two that brings
@@ -66,10 +59,8 @@ struct TravCfg {
 // FP8 E4M3: rows are stored divided by per-dimension scales (largest
 // magnitude onto 448); a query is multiplied by the same scales, brought into
 // E4M3's range by a power of two, and stored as two E4M3 parts - its rounding
-// and the rounding of the remainder - so that two products recover it to
-// about 0.02% per component; the power of two is undone after the product.
-template <int TRAV, int KT>
-struct TravQuery {};
+// and the rounding of the remainder - which together recover it to about
+// 0.02% per component; the power of two is undone after the product.
 
 struct TravView {
     const uint8_t *rows;      // traversal copy, row_bytes apart
@@ -193,8 +184,8 @@ __device__ __forceinline__ void mma_step(float (&c)[4], const uint32_t (&a)[4], 
 // staged query) in column 1 (lanes 4-7), so one product per k-step yields
 // both; a row's dot product is columns 0 + 1, scaled by qfac.
 // L2 = |q|^2 + |x|^2 - 2 q.x from the stored norms of the same values.
-template <int TRAV, int KT>
-__device__ __forceinline__ void trav_dist_buf(const TravCfg &, const TravQuery<TRAV, KT> &, bool ip, float qnorm,
+template <int TRAV>
+__device__ __forceinline__ void trav_dist_buf(bool ip, float qnorm,
                                               float qfac, const RowFetch &f, int64_t data_bytes, const uint8_t *qbuf,
                                               float *cd, int n, int lane) {
     auto xnorm = [&](int t) { return *reinterpret_cast<const float *>(f.buf + t * f.stride + data_bytes); };
@@ -423,9 +414,9 @@ __device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, i
 // ------------------------------------------------------------------ walk ---
 // Narrow lists (ef <= 128) fit 80 registers per thread without spills, so
 // three 256-thread blocks can be resident per SM; wider lists take two.
-template <int TRAV, int KT, int S>
+template <int TRAV, int S>
 __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
-    walk_kernel(const DevGraph *__restrict__ gp, const TravCfg tc, const WalkArgs a) {
+    walk_kernel(const DevGraph *__restrict__ gp, const WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -467,7 +458,6 @@ __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
         const int L = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, 32 * S));
 
         // the query in the traversal format, staged in shared memory
-        TravQuery<TRAV, KT> tq;
         const float qnorm = ip ? 0.f : a.qnorm[q];
         float qfac = 1.f;
         {
@@ -494,13 +484,13 @@ __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
                 failed = true;
                 break;
             }
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
+            trav_dist_buf<TRAV>(ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
             float best = cd[0];
             int32_t c = enter;
             bool moved = false;
             auto flush_up = [&](int nn) -> bool {
                 if (!fetch_rows(f, tv, crow, nn, lane)) return false;
-                trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, nn, lane);
+                trav_dist_buf<TRAV>(ip, qnorm, qfac, f, tdb, qbuf, cd, nn, lane);
                 float bd;
                 int bt;
                 warp_argmin(cd, nn, bd, bt, lane);
@@ -550,7 +540,7 @@ __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
             if (!fetch_rows(f, tv, crow, 1, lane)) failed = true;
         }
         if (!failed) {
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
+            trav_dist_buf<TRAV>(ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
             const float d0 = cd[0];
             if (lane == 0) {
                 list.d[0] = d0;
@@ -562,7 +552,7 @@ __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
         }
         auto flush0 = [&](int nn) -> bool {
             if (!fetch_rows(f, tv, crow, nn, lane)) return false;
-            trav_dist_buf<TRAV, KT>(tc, tq, ip, qnorm, qfac, f, tdb, qbuf, cd, nn, lane);
+            trav_dist_buf<TRAV>(ip, qnorm, qfac, f, tdb, qbuf, cd, nn, lane);
             cnt[4] += nn;
             for (int i0 = 0; i0 < nn; i0 += 32) {
                 const int i = i0 + lane;
@@ -750,23 +740,23 @@ __global__ void bin_by_slots_kernel(const int32_t *ef_arr, int32_t ef_bound, int
 }
 
 // ------------------------------------------------------------ dispatch -----
-template <int TRAV, int KT>
+template <int TRAV>
 void *walk_pick_s(int s) {
     switch (s) {
-        case 1: return (void *)walk_kernel<TRAV, KT, 1>;
-        case 2: return (void *)walk_kernel<TRAV, KT, 2>;
-        case 3: return (void *)walk_kernel<TRAV, KT, 3>;
-        case 4: return (void *)walk_kernel<TRAV, KT, 4>;
-        case 6: return (void *)walk_kernel<TRAV, KT, 6>;
-        case 8: return (void *)walk_kernel<TRAV, KT, 8>;
-        case 12: return (void *)walk_kernel<TRAV, KT, 12>;
-        case 16: return (void *)walk_kernel<TRAV, KT, 16>;
+        case 1: return (void *)walk_kernel<TRAV, 1>;
+        case 2: return (void *)walk_kernel<TRAV, 2>;
+        case 3: return (void *)walk_kernel<TRAV, 3>;
+        case 4: return (void *)walk_kernel<TRAV, 4>;
+        case 6: return (void *)walk_kernel<TRAV, 6>;
+        case 8: return (void *)walk_kernel<TRAV, 8>;
+        case 12: return (void *)walk_kernel<TRAV, 12>;
+        case 16: return (void *)walk_kernel<TRAV, 16>;
         default: return nullptr;
     }
 }
-void *walk_kernel_ptr(int trav, int kt, int s) {
-    if (trav == kTravF16) return kt == 1 ? walk_pick_s<kTravF16, 1>(s) : nullptr;
-    if (trav == kTravE4M3) return kt == 1 ? walk_pick_s<kTravE4M3, 1>(s) : nullptr;
+void *walk_kernel_ptr(int trav, int s) {
+    if (trav == kTravF16) return walk_pick_s<kTravF16>(s);
+    if (trav == kTravE4M3) return walk_pick_s<kTravE4M3>(s);
     return nullptr;
 }
 
@@ -924,19 +914,8 @@ __global__ void prep_queries_kernel(const uint8_t *q, int64_t row_bytes, int64_t
 
 }  // namespace
 
-TravCfgHost trav_config(int64_t trav_data_bytes, int trav) {
-    // both formats run on the tensor cores with the query in shared memory;
-    // one instantiation per list width
-    TravCfgHost t;
-    t.CT = (int)(trav_data_bytes / 16);
-    t.GT = 32;
-    t.KT = 1;
-    t.KTMAX = trav == kTravF16 || trav == kTravE4M3 ? 1 : 0;
-    return t;
-}
-
-int walk_blocks_per_sm(int trav, const TravCfgHost &tc, int slots, int wpb, size_t smem) {
-    void *fn = walk_kernel_ptr(trav, tc.KTMAX, slots);
+int walk_blocks_per_sm(int trav, int slots, int wpb, size_t smem) {
+    void *fn = walk_kernel_ptr(trav, slots);
     if (!fn) return 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
@@ -944,14 +923,13 @@ int walk_blocks_per_sm(int trav, const TravCfgHost &tc, int slots, int wpb, size
     return nb;
 }
 
-cudaError_t launch_walk(const DevGraph *g, int trav, const TravCfgHost &tch, int slots, const WalkArgs &a, int grid,
-                        int wpb, size_t smem, cudaStream_t s) {
-    void *fn = walk_kernel_ptr(trav, tch.KTMAX, slots);
+cudaError_t launch_walk(const DevGraph *g, int trav, int slots, const WalkArgs &a, int grid, int wpb, size_t smem,
+                        cudaStream_t s) {
+    void *fn = walk_kernel_ptr(trav, slots);
     if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    TravCfg tc{tch.GT, tch.KT, tch.CT};
-    void *args[] = {(void *)&g, (void *)&tc, (void *)&a};
+    void *args[] = {(void *)&g, (void *)&a};
     return cudaLaunchKernel(fn, dim3(grid), dim3(wpb * 32), args, smem, s);
 }
 

@@ -10,11 +10,6 @@ constexpr int kTravE4M3 = 2;  // traversal copy in FP8 E4M3 with per-dimension s
 
 constexpr int kFastMaxEf = 512;  // the walk's register list holds up to 32 * 16 entries
 
-struct TravCfgHost {
-    int GT, KT, CT, KTMAX;
-};
-TravCfgHost trav_config(int64_t trav_data_bytes, int trav);
-
 // Bytes of a traversal query row: FP16 = the values; E4M3 = the query's two
 // E4M3 parts and a 16-byte chunk holding its power-of-two factor.
 __host__ __device__ inline int64_t trav_query_bytes(int trav, int64_t trav_data_bytes) {
@@ -142,13 +137,13 @@ __host__ __device__ inline int slot_class(int ef) {
 }
 __host__ __device__ inline int list_slots(int ef) { return slot_class_width(slot_class(ef)); }
 
-int walk_blocks_per_sm(int trav, const TravCfgHost &tc, int slots, int wpb, size_t smem);
+int walk_blocks_per_sm(int trav, int slots, int wpb, size_t smem);
 // Sorts the queries by list width class: lists[c * nq + i] = the i-th query
 // of class c, counts[c] = how many (counts zeroed by the caller).
 cudaError_t launch_bin_by_slots(const int32_t *ef_arr, int32_t ef_bound, int64_t nq, int32_t *counts,
                                 int32_t *lists, cudaStream_t s);
-cudaError_t launch_walk(const DevGraph *g, int trav, const TravCfgHost &tc, int slots, const WalkArgs &a, int grid,
-                        int wpb, size_t smem, cudaStream_t s);
+cudaError_t launch_walk(const DevGraph *g, int trav, int slots, const WalkArgs &a, int grid, int wpb, size_t smem,
+                        cudaStream_t s);
 int rerank_blocks_per_sm(int dtype, const LaneCfg &lc, int wpb, size_t smem);
 cudaError_t launch_rerank(const DevGraph *g, int dtype, const LaneCfg &lc, const RerankArgs &a, int grid, int wpb,
                           size_t smem, cudaStream_t s);

@@ -854,7 +854,6 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     const bool binned = ef_arr != nullptr && slots > 1;
     WalkShape ws;
     PK_TRY(walk_shape(h, ws));
-    const pk::TravCfgHost tc = pk::trav_config(h->trav_data_bytes, h->trav);
     PK_TRY(ensure_buf(h, &c.d_work, c.work_n, kWorkInts));
     PK_TRY(ensure_buf(h, &c.d_cand, c.cand_n, nq * cs));
     if (binned) PK_TRY(ensure_buf(h, &c.d_lists, c.lists_n, nq * pk::kSlotClasses));
@@ -905,13 +904,13 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
         const int sl = pk::slot_class_width(cls);
         if (!binned && sl != slots) continue;
-        const int nb = pk::walk_blocks_per_sm(h->trav, tc, sl, ws.wpb, ws.smem);
+        const int nb = pk::walk_blocks_per_sm(h->trav, sl, ws.wpb, ws.smem);
         if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
         const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + ws.wpb - 1) / ws.wpb);
         a.work = c.d_work + kWorkCounters + cls;
         a.qlist = binned ? c.d_lists + cls * nq : nullptr;
         a.qcount = binned ? c.d_work + kWorkCounts + cls : nullptr;
-        PK_CUDA(pk::launch_walk(h->dg, h->trav, tc, sl, a, (int)grid, ws.wpb, ws.smem, s));
+        PK_CUDA(pk::launch_walk(h->dg, h->trav, sl, a, (int)grid, ws.wpb, ws.smem, s));
     }
     if (timed) PK_CUDA(cudaEventRecord(c.ev[1], s));
 
