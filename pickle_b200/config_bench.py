@@ -71,8 +71,9 @@ def traversal_copy(base, queries, path):
     same rules: FP16 = values divided by the power of two sc with
     max|x| / sc in [4, 8) (queries clamped to 64 in those units); FP8 E4M3 =
     values divided by per-dimension max|x| / 448, rounded to E4M3 and scaled
-    back (queries stay in full precision).  Returns (rows, queries) as
-    float64 in original units."""
+    back (queries in full precision: the kernel's two E4M3 query parts carry a
+    query to about 0.02% per component).  Returns (rows, queries) as float64
+    in original units."""
     import torch
     amax = np.abs(base.astype(np.float32)).max(0)
     if path == "f16":

@@ -1416,18 +1416,22 @@ static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq,
         }
         return true;
     };
-    // stage 1: visited-table size and warps per block at 32 rows per batch
-    // (the table trades re-fetched rows against occupancy, more so as ef
-    // grows); stage 2: rows per batch at the best pair
+    // stage 1: visited-table size and warps per block at 16 and at 32 rows
+    // per batch (the table trades re-fetched rows against occupancy, more so
+    // as ef grows, and the staged rows share the same shared memory: large
+    // rows at 32 per batch leave room only for small tables); stage 2: rows
+    // per batch at the best triple
     const int hls[] = {8, 9, 10, 11, 12, 13};
     const int wps[] = {1, 2, 4};
-    for (int hl : hls)
-        for (int wp : wps)
-            if (rc == PK_OK) time_shape(32, hl, wp);
-    const int h1 = bh, w1 = bw;
-    const int rbs[] = {16, 24, 48, 64};
+    const int rbs1[] = {16, 32};
+    for (int rb : rbs1)
+        for (int hl : hls)
+            for (int wp : wps)
+                if (rc == PK_OK) time_shape(rb, hl, wp);
+    const int r1 = brb, h1 = bh, w1 = bw;
+    const int rbs[] = {8, 16, 24, 32, 48, 64};
     for (int rb : rbs)
-        if (rc == PK_OK && best >= 0.f) time_shape(rb, h1, w1);
+        if (rc == PK_OK && best >= 0.f && rb != r1) time_shape(rb, h1, w1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc == PK_OK) rc = fast_status(h, h->fctx, s);
