@@ -44,7 +44,7 @@ CONFIGS = {
     "c1": dict(n=100_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256]),
     "c3u8": dict(n=1_000_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256]),
     "c3i8": dict(n=1_000_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256]),
-    "c4": dict(n=10_000_000, nq=100_000, dim=128, metric="l2", M=32, efc=200, efs=[16, 24, 32, 48, 64, 96, 128],
+    "c4": dict(n=10_000_000, nq=100_000, dim=128, metric="l2", M=32, efc=200, efs=[16, 24, 32, 48, 64, 96, 112, 128],
                mixed=True),
 }
 
