@@ -414,7 +414,10 @@ __device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, i
 // ------------------------------------------------------------------ walk ---
 // Narrow lists (ef <= 128) fit 80 registers per thread without spills, so
 // three 256-thread blocks can be resident per SM; wider lists take two.
-template <int TRAV, int S>
+// EXP bounds the parents expanded per step: the walk with one parent per
+// step (the default) has its own instantiation, a quarter of the layer-0
+// loop's code of the one that takes up to four.
+template <int TRAV, int S, int EXP>
 __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
     walk_kernel(const DevGraph *__restrict__ gp, const WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -443,7 +446,7 @@ __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
     const int64_t tdb = a.trav_data_bytes;
     const int enter_level = gp->enter_level;
     const int rb = a.rb;
-    const int expand = max(1, min(a.expand, 4));
+    const int expand = max(1, min(a.expand, EXP));
     const DevLayer L0 = gp->L[0];
     const int64_t lim0 = min(L0.lcap, a.trav_rows);
     const float kInf = __int_as_float(0x7f800000);
@@ -580,13 +583,13 @@ __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
         while (!failed) {
             int32_t pc[4];
 #pragma unroll
-            for (int p = 0; p < 4; p++) pc[p] = p < expand ? list.take_first(vmask, lane) : -1;
+            for (int p = 0; p < 4; p++) pc[p] = p < EXP && p < expand ? list.take_first(vmask, lane) : -1;
             if (pc[0] < 0 || ++iters > L0.lcap) break;
             // degrees and the first 64 slots of each parent's list, all in flight
             int pdeg[4];
             int32_t pa0[4], pa1[4];
 #pragma unroll
-            for (int p = 0; p < 4; p++) {
+            for (int p = 0; p < EXP; p++) {
                 pdeg[p] = 0;
                 pa0[p] = -1;
                 pa1[p] = -1;
@@ -599,7 +602,7 @@ __global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
             }
             int n = 0;
 #pragma unroll
-            for (int p = 0; p < 4; p++) {
+            for (int p = 0; p < EXP; p++) {
                 if (pc[p] < 0 || failed) continue;
                 const int deg = pdeg[p];
                 const int64_t base = (int64_t)pc[p] * L0.cap;
@@ -740,23 +743,23 @@ __global__ void bin_by_slots_kernel(const int32_t *ef_arr, int32_t ef_bound, int
 }
 
 // ------------------------------------------------------------ dispatch -----
-template <int TRAV>
+template <int TRAV, int EXP>
 void *walk_pick_s(int s) {
     switch (s) {
-        case 1: return (void *)walk_kernel<TRAV, 1>;
-        case 2: return (void *)walk_kernel<TRAV, 2>;
-        case 3: return (void *)walk_kernel<TRAV, 3>;
-        case 4: return (void *)walk_kernel<TRAV, 4>;
-        case 6: return (void *)walk_kernel<TRAV, 6>;
-        case 8: return (void *)walk_kernel<TRAV, 8>;
-        case 12: return (void *)walk_kernel<TRAV, 12>;
-        case 16: return (void *)walk_kernel<TRAV, 16>;
+        case 1: return (void *)walk_kernel<TRAV, 1, EXP>;
+        case 2: return (void *)walk_kernel<TRAV, 2, EXP>;
+        case 3: return (void *)walk_kernel<TRAV, 3, EXP>;
+        case 4: return (void *)walk_kernel<TRAV, 4, EXP>;
+        case 6: return (void *)walk_kernel<TRAV, 6, EXP>;
+        case 8: return (void *)walk_kernel<TRAV, 8, EXP>;
+        case 12: return (void *)walk_kernel<TRAV, 12, EXP>;
+        case 16: return (void *)walk_kernel<TRAV, 16, EXP>;
         default: return nullptr;
     }
 }
-void *walk_kernel_ptr(int trav, int s) {
-    if (trav == kTravF16) return walk_pick_s<kTravF16>(s);
-    if (trav == kTravE4M3) return walk_pick_s<kTravE4M3>(s);
+void *walk_kernel_ptr(int trav, int s, int expand) {
+    if (trav == kTravF16) return expand > 1 ? walk_pick_s<kTravF16, 4>(s) : walk_pick_s<kTravF16, 1>(s);
+    if (trav == kTravE4M3) return expand > 1 ? walk_pick_s<kTravE4M3, 4>(s) : walk_pick_s<kTravE4M3, 1>(s);
     return nullptr;
 }
 
@@ -914,8 +917,8 @@ __global__ void prep_queries_kernel(const uint8_t *q, int64_t row_bytes, int64_t
 
 }  // namespace
 
-int walk_blocks_per_sm(int trav, int slots, int wpb, size_t smem) {
-    void *fn = walk_kernel_ptr(trav, slots);
+int walk_blocks_per_sm(int trav, int slots, int expand, int wpb, size_t smem) {
+    void *fn = walk_kernel_ptr(trav, slots, expand);
     if (!fn) return 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
@@ -925,7 +928,7 @@ int walk_blocks_per_sm(int trav, int slots, int wpb, size_t smem) {
 
 cudaError_t launch_walk(const DevGraph *g, int trav, int slots, const WalkArgs &a, int grid, int wpb, size_t smem,
                         cudaStream_t s) {
-    void *fn = walk_kernel_ptr(trav, slots);
+    void *fn = walk_kernel_ptr(trav, slots, a.expand);
     if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -137,7 +137,7 @@ __host__ __device__ inline int slot_class(int ef) {
 }
 __host__ __device__ inline int list_slots(int ef) { return slot_class_width(slot_class(ef)); }
 
-int walk_blocks_per_sm(int trav, int slots, int wpb, size_t smem);
+int walk_blocks_per_sm(int trav, int slots, int expand, int wpb, size_t smem);
 // Sorts the queries by list width class: lists[c * nq + i] = the i-th query
 // of class c, counts[c] = how many (counts zeroed by the caller).
 cudaError_t launch_bin_by_slots(const int32_t *ef_arr, int32_t ef_bound, int64_t nq, int32_t *counts,

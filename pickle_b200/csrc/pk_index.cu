@@ -904,7 +904,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
         const int sl = pk::slot_class_width(cls);
         if (!binned && sl != slots) continue;
-        const int nb = pk::walk_blocks_per_sm(h->trav, sl, ws.wpb, ws.smem);
+        const int nb = pk::walk_blocks_per_sm(h->trav, sl, a.expand, ws.wpb, ws.smem);
         if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
         const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + ws.wpb - 1) / ws.wpb);
         a.work = c.d_work + kWorkCounters + cls;
