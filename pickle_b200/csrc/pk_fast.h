@@ -125,7 +125,7 @@ __host__ __device__ inline RerankLayout rerank_layout(int cand_stride, int64_t r
 
 // List widths: slots per lane of the register list, which holds 32 entries
 // per slot.  A query takes the narrowest width that holds its ef, so its list
-// is at most a third wider than ef.
+// is at most twice ef (ef <= 64) or half again as wide (ef > 64).
 constexpr int kSlotClasses = 8;
 __host__ __device__ inline int slot_class_width(int c) {
     return c < 3 ? c + 1 : c == 3 ? 4 : c == 4 ? 6 : c == 5 ? 8 : c == 6 ? 12 : 16;  // 1 2 3 4 6 8 12 16
