@@ -8,9 +8,9 @@
 // suited to a warp, and are judged by recall.  Two launches per batch:
 //
 // walk_kernel (one query per warp, work stealing, per-query ef):
-//   * traversal distances come from a low-precision copy of the vectors:
-//     FP16 (dot products on the tensor cores), or FP8 E4M3 scaled per
-//     dimension (a query is scaled by the same per-dimension factors); for L2
+//   * traversal distances come from a low-precision copy of the vectors,
+//     FP16 or FP8 E4M3 scaled per dimension (a query is scaled by the same
+//     per-dimension factors), as dot products on the tensor cores; for L2
 //     each row carries its stored norm (after its values), which turns the
 //     distance into a dot product;
 //   * upper layers are descended greedily as in SlideLayer
