@@ -229,8 +229,10 @@ int pk_index_search_noalloc(const pk_index *h, const void *queries, int64_t nq, 
 
 /* Replaces the Serializer::to_disk / from_disk pair that the reference names
  * for persistence (include/serializer.hpp:21-25) but only implements for its
- * retired v0 layer.  Writes / reads the v2 graph file (format described in
- * DESIGN.md and pickle_b200/csrc/pk_format.cpp). */
+ * retired v0 layer.  Writes / reads the v2 graph file: a versioned header,
+ * per layer the reference's record layout (include/serializer.hpp:27-55)
+ * extended with the v2 layer's fields, the layer-0 vectors and a checksum (the
+ * byte layout is written out in pickle_b200/csrc/pk_format.cpp). */
 int pk_index_save(const pk_index *h, const char *path);
 int pk_index_load(pk_index **out, const char *path);
 
