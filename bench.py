@@ -1,35 +1,56 @@
-"""QPS at recall@10 >= 0.95 for HNSW search on one B200 (and N replicas).
+"""HNSW search throughput on one B200 (and N replicas), low-precision walk with
+exact re-rank against the plain exact search.
 
-Workload (the configuration the headline metric is quoted on): 1M base
-vectors, dim 96, float32, unit-normalised rows from a 256-component Gaussian
-mixture (sigma 0.3 around random unit centres), inner product, M = 32,
-ef_construction = 400; 10k queries from the same mixture, k = 10.  Data are
-seeded synthetic stand-ins (the public datasets are not available offline).
-ef is the smallest value of a fixed sweep whose recall@10 against exact
-(float64) ground truth reaches 0.95.
+Workload (default, the configuration the target is stated on): 10M base
+vectors, dim 128, stored as float16, from a 1024-component Gaussian mixture
+(unit-normal centres, sigma 0.5); L2; M = 32, ef_construction = 200, graph
+built on the GPU; one batch of 100k queries from the same mixture, each with
+its own k uniform in {1, 10, 100} and ef uniform in [max(k, 16), 512].  Seeded
+synthetic stand-ins (the public datasets are not available offline).
 
-A step is one batch search of the 10k queries.
-  value   device-resident: queries and results in HBM, CUDA events around each
-          pk_index_search_device call on its stream, L2 flushed between steps.
-  e2e     through the C ABI with host buffers (pk_index_search): pinned host
-          queries in, ids and distances out, copies inside the timed region.
-  roofline  algorithmic bytes per launch (distance rows read + adjacency rows
-          read, from the device's own work counters) over the kernel's average
-          duration, against the measured HBM copy bandwidth.
+A step is one search of the whole 100k-query batch.
+  value   device-resident queries/s of the best path on the mixed batch: CUDA
+          events around each search on its stream; the index (10.7 GB) is far
+          larger than L2, and a 256 MiB buffer is written between steps.
+  e2e     the same batch through the C ABI with host buffers
+          (pk_index_search_fast_host_var / pk_index_search): pinned host
+          queries and per-query k/ef in, ids and distances out, copies inside
+          the timed region.
+  config.paths  per path (exact = the drop-in search that replays the
+          reference's heaps; f16 / fp8 = low-precision walk + exact re-rank):
+          the mixed batch, and the recall@10 >= 0.95 point of a k = 10 ef
+          sweep (recall on a 10k-query sample against float64 ground truth,
+          QPS on the whole batch), each with its speed-up over the exact path.
+  roofline  the walk kernel: algorithmic bytes per query (distinct traversal
+          rows x their value bytes + adjacency rows read; the per-query work
+          counters with a table large enough to forget nothing) x queries /
+          the walk launches' device time (events the library records around
+          them on the bench's stream), against the measured HBM bandwidth.
   cpu_baseline  the reference's own search (oracle/_ref/pk_ref, all host
-          threads) on the same saved graph, on a bounded sample of the queries.
+          threads) on the same graph file, on a 2000-query sample of the
+          mixed batch (its own k and ef per query).
 
---impl reference runs the reference's own build and search on the host cores
-instead (rank 0 only) and prints the same line with impl = reference.
+--impl reference runs the reference's search on the host cores instead
+(rank 0 only) on the same sample and prints the same line with impl =
+reference.  Its graph is the GPU-built one (a reference Build of 10M rows
+takes hours on the host); both arms share it through a file cache.
 
-Multi-GPU (torchrun, one process per GPU): every rank holds a full replica and
-searches its own 10k queries; no collective is on the data path (weak scaling).
+--workload c2 runs the earlier configuration instead: 1M x 96 float32 unit
+rows (256-component mixture, sigma 0.3), inner product, M = 32, efC = 400,
+10k queries, k = 10, and reports QPS at the smallest ef of a sweep with
+recall@10 >= 0.95.
+
+Multi-GPU (--gpus N; relaunches itself under torch.distributed.run when
+WORLD_SIZE is unset): every rank holds a full replica and searches its own
+batch; no collective is on the data path (weak scaling).
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -42,9 +63,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC_NAME = "QPS at recall@10>=0.95 (1M x 96 f32, IP, M=32, efC=400, k=10)"
-EF_SWEEP = [16, 24, 32, 36, 40, 44, 48, 56, 64, 80, 96, 112, 128, 160, 192, 256, 320, 384, 512]
 RECALL_TARGET = 0.95
+WORKLOADS = {
+    "c4": dict(n=10_000_000, nq=100_000, dim=128, dtype="f16", metric="l2", M=32, efc=200, mixed=True,
+               sweep=[32, 48, 64, 80, 96, 112, 128, 160, 192, 256], sample=10_000),
+    "c2": dict(n=1_000_000, nq=10_000, dim=96, dtype="f32", metric="ip", M=32, efc=400, mixed=False,
+               sweep=[16, 24, 32, 36, 40, 44, 48, 56, 64, 80, 96, 112, 128, 160, 192, 256, 320, 384, 512],
+               sample=10_000),
+}
 
 
 def parse():
@@ -53,19 +79,19 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--n", type=int, default=1_000_000)
-    p.add_argument("--nq", type=int, default=10_000)
-    p.add_argument("--dim", type=int, default=96)
-    p.add_argument("--M", type=int, default=32)
-    p.add_argument("--efc", type=int, default=400)
-    p.add_argument("--k", type=int, default=10)
+    p.add_argument("--workload", default="c4", choices=sorted(WORKLOADS))
+    p.add_argument("--n", type=int, default=0, help="base rows (default: the workload's)")
+    p.add_argument("--nq", type=int, default=0, help="queries per GPU (default: the workload's)")
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-sample", type=int, default=2000, help="queries in the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--verbose", action="store_true")
-    p.add_argument("--paths", default="exact,f16,fp8", help="search paths to measure (exact, f16, fp8)")
+    p.add_argument("--paths", default="exact,f16", help="search paths to measure (exact, f16, fp8)")
     p.add_argument("--expand", type=int, default=1, help="entries expanded per step on the fast paths")
     p.add_argument("--fast-shape", default="", help="rows,filter_log2,warps for the fast walk instead of tuning")
+    p.add_argument("--cache", default=os.environ.get("PK_BENCH_CACHE", os.path.join(tempfile.gettempdir(),
+                                                                                   "pickle_b200_bench")),
+                   help="directory for the built graph file, shared by both arms ('' = no cache)")
     return p.parse_args()
 
 
@@ -74,33 +100,108 @@ def log(args, *a):
         print(*a, file=sys.stderr, flush=True)
 
 
-def make_data(args, rank):
+def workload(args):
+    w = dict(WORKLOADS[args.workload])
+    if args.n:
+        w["n"] = args.n
+    if args.nq:
+        w["nq"] = args.nq
+    w["sample"] = min(w["sample"], w["nq"])
+    return w
+
+
+def workload_name(w):
+    t = {"f16": "float16", "f32": "float32"}[w["dtype"]]
+    s = f"{w['n'] // 1_000_000}M x {w['dim']} {t}, {w['metric'].upper()}, M={w['M']}, efC={w['efc']}, "
+    if w["mixed"]:
+        return s + f"{w['nq'] // 1000}k queries per GPU, k in {{1,10,100}}, ef in [max(k,16),512] per query"
+    return s + f"{w['nq'] // 1000}k queries per GPU, k=10, smallest ef with recall@10>=0.95"
+
+
+def metric_name(w):
+    if w["mixed"]:
+        return f"QPS of one {w['nq'] // 1000}k-query batch with per-query k and ef ({workload_name(w)})"
+    return f"QPS at recall@10>=0.95 ({workload_name(w)})"
+
+
+def make_data(w, seed, rank):
     from pickle_b200 import datasets
-    base, _ = datasets.gmm_unit(args.n, 0, args.dim, ncomp=256, sigma=0.3, seed=args.seed)
-    # every rank has its own 10k queries from the same mixture
-    _, queries = datasets.gmm_unit(0, args.nq, args.dim, ncomp=256, sigma=0.3, seed=args.seed)
+    if w["dtype"] == "f16":
+        base, queries = datasets.gmm_f16(w["n"], w["nq"], w["dim"], ncomp=1024, sigma=0.5, seed=seed)
+    else:
+        base, queries = datasets.gmm_unit(w["n"], w["nq"], w["dim"], ncomp=256, sigma=0.3, seed=seed)
     if rank:
-        rng = np.random.default_rng(1000 + rank)
-        queries = queries[rng.permutation(len(queries))]
+        queries = queries[np.random.default_rng(1000 + rank).permutation(len(queries))]
     return base, queries
 
 
-def ground_truth(base, queries, k, device):
-    """Exact top-k by inner product: float32 candidates, float64 rescoring."""
+def per_query_k_ef(w, nq, seed):
+    """k uniform in {1, 10, 100}, ef uniform in [max(k, 16), 512] (mixed), else k = 10."""
+    rng = np.random.default_rng(seed + 7)
+    if not w["mixed"]:
+        return np.full(nq, 10, np.int32), None
+    kq = rng.choice([1, 10, 100], size=nq).astype(np.int32)
+    efq = np.array([rng.integers(max(int(k), 16), 513) for k in kq], np.int32)
+    return kq, efq
+
+
+def recall_mixed(found, truth, ks):
+    hit = 0
+    for f, t, k in zip(found, truth, ks):
+        hit += len(set(int(x) for x in f[:k] if x >= 0) & set(int(x) for x in t[:k]))
+    return hit / float(np.sum(ks))
+
+
+def lib_digest():
+    from pickle_b200 import LIB_PATH
+    h = hashlib.sha1()
+    with open(LIB_PATH, "rb") as f:
+        for blk in iter(lambda: f.read(1 << 22), b""):
+            h.update(blk)
+    return h.hexdigest()[:16]
+
+
+def graph_file(args, w):
+    if not args.cache:
+        return None
+    key = f"{args.workload}_{w['n']}_{w['dim']}_{args.seed}_{lib_digest()}"
+    return os.path.join(args.cache, key + ".pkg")
+
+
+def build_or_load(args, w, base, rank):
+    """The GPU-built graph: loaded from the cache file when a run with the same
+    workload, seed and library built it already, else built (and, on rank 0,
+    saved).  Returns (index, build seconds or None, path of a saved copy or None)."""
     import torch
-    torch.backends.cuda.matmul.allow_tf32 = False
-    b = torch.from_numpy(base).to(device)
-    out = np.empty((len(queries), k), np.int64)
-    cand = 64
-    for i in range(0, len(queries), 1024):
-        q = torch.from_numpy(queries[i:i + 1024]).to(device)
-        s = q @ b.T
-        top = torch.topk(s, cand, dim=1).indices
-        s64 = (q.double()[:, None, :] * b[top].double()).sum(-1)
-        order = torch.argsort(-s64, dim=1, stable=True)[:, :k]
-        out[i:i + 1024] = torch.gather(top, 1, order).cpu().numpy()
-    del b
-    return out
+
+    from pickle_b200 import HNSWIndex
+    path = graph_file(args, w)
+    if path and os.path.exists(path):
+        try:
+            t0 = time.time()
+            idx = HNSWIndex.load(path)
+            log(args, f"[{rank}] loaded {path} in {time.time() - t0:.1f}s")
+            return idx, None, path
+        except Exception as e:  # a partial or stale file: build instead
+            log(args, f"[{rank}] cache load failed ({e}); building")
+    idx = HNSWIndex(w["dim"], base.dtype, w["metric"], M=w["M"], ef_construction=w["efc"])
+    idx.set_seed(args.seed)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    idx.build(base)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    saved = None
+    if path and rank == 0:
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            tmp = path + f".tmp{os.getpid()}"
+            idx.save(tmp)
+            os.replace(tmp, path)
+            saved = path
+        except Exception as e:
+            log(args, f"cache save failed: {e}")
+    return idx, build_s, saved
 
 
 class ClockSampler:
@@ -167,27 +268,39 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_query(kernel):
-    """DRAM bytes per query of a kernel from its committed ncu summary."""
+def profiled_traffic(workload_key, path):
+    """DRAM bytes per query of the walk from a committed ncu summary of the
+    same workload and path (a figure of that capture, not of this run)."""
     try:
-        with open(os.path.join(ROOT, "profiles", f"{kernel}_1Mx96_traffic.json")) as f:
-            return json.load(f)
+        with open(os.path.join(ROOT, "profiles", f"walk_kernel_{workload_key}_traffic.json")) as f:
+            d = json.load(f)
+        return d if d.get("path") == path else None
     except (OSError, ValueError):
         return None
 
 
-def cpu_baseline(args, graph_path, queries, ef):
-    """The reference's AnnSearch on the saved graph, all host threads, on a bounded sample."""
+def cpu_reference(graph_path, queries, k, ef, kq, efq, repeat, warmup=0):
+    """The reference's AnnSearch on a graph file, all host threads; returns
+    (per-run seconds after the warm-up runs, threads)."""
     import oracle
-    if not oracle.ref_available():
-        return None
-    sample = queries[: args.cpu_sample]
     threads = os.cpu_count() or 1
-    _, _, info = oracle.ref_search(graph_path, sample, args.k, ef, threads=threads, repeat=3, want_results=False)
-    return {"value": round(info["qps"], 1), "unit": "queries/s", "cores": threads, "kind": "reference",
-            "sample": f"{len(sample)} of the {len(queries)} queries at ef={ef}, same graph file, median of 3 batch "
-                      f"AnnSearch runs (steady clock around the batch)"}
+    _, _, info = oracle.ref_search(graph_path, queries, k, ef, threads=threads, repeat=warmup + repeat,
+                                   want_results=False, k_per_query=kq, ef_per_query=efq)
+    return info["all_s"][warmup:], threads
 
+
+def relaunch_distributed(args):
+    """--gpus N without a torch.distributed environment: rerun this command
+    under torch.distributed.run with N processes on this node."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+# -------------------------------------------------------------------- ours --
 
 def run_ours(args):
     import ctypes
@@ -195,103 +308,55 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    from pickle_b200 import HNSWIndex, datasets, lib
+    from pickle_b200 import datasets, lib
+    from pickle_b200.groundtruth import gpu_knn
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE is {world}")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(minutes=30), device_id=dev)
 
-    base, queries = make_data(args, rank)
+    w = workload(args)
+    base, queries = make_data(w, args.seed, rank)
+    nq = len(queries)
     log(args, f"[{rank}] data ready")
-    idx = HNSWIndex(args.dim, np.float32, "ip", M=args.M, ef_construction=args.efc)
-    idx.set_seed(args.seed)
-    t0 = time.time()
-    idx.build(base)
-    torch.cuda.synchronize()
-    build_s = time.time() - t0
-    log(args, f"[{rank}] build {build_s:.1f}s")
-    gt = ground_truth(base, queries, args.k, dev)
+    idx, build_s, saved = build_or_load(args, w, base, rank)
+    log(args, f"[{rank}] index ready (build {build_s})")
+    kq, efq = per_query_k_ef(w, nq, args.seed)
+    kmax = int(kq.max())
+    ns = w["sample"]
+    gt = gpu_knn(base, queries[:ns], max(kmax, 10), w["metric"], dev)
+    del base
 
-    nq, k = len(queries), args.k
     q_dev = torch.from_numpy(queries).to(dev)
-    ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
-    ds = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    kq_dev = torch.from_numpy(kq).to(dev)
+    efq_dev = torch.from_numpy(efq).to(dev) if efq is not None else None
+    ids = torch.empty((nq, kmax), dtype=torch.int32, device=dev)
+    ds = torch.empty((nq, kmax), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB of L2
     L = lib()
-    qh = torch.from_numpy(queries).pin_memory()
-    ih = torch.empty((nq, k), dtype=torch.int32).pin_memory()
-    dh = torch.empty((nq, k), dtype=torch.float32).pin_memory()
 
-    def call(path, ef, counters=None):
+    def call(path, k, ef, mixed, counters=None, q=q_dev, out_i=ids, out_d=ds):
+        kk = kq_dev[:q.shape[0]] if mixed else None
+        ee = efq_dev[:q.shape[0]] if mixed else None
         if path == "exact":
-            idx.search_device(q_dev, k, ef, ids, ds, counters=counters, stream=stream)
+            idx.search_device(q, k, ef, out_i, out_d, k_per_query=kk, ef_per_query=ee, counters=counters,
+                              stream=stream)
         else:
-            idx.search_fast_device(q_dev, k, ef, ids, ds, counters=counters, expand=args.expand, stream=stream)
+            idx.search_fast_device(q, k, ef, out_i, out_d, k_per_query=kk, ef_per_query=ee, counters=counters,
+                                   expand=args.expand, stream=stream)
 
-    def host_call(path, ef):
-        qp, ip_, dp = (ctypes.c_void_p(t.data_ptr()) for t in (qh, ih, dh))
-        if path == "exact":
-            rc = L.pk_index_search(idx._h, qp, nq, k, ef, ip_, dp)
-        else:
-            rc = L.pk_index_search_fast_host(idx._h, qp, nq, k, ef, ip_, dp, args.expand)
-        if rc != 0:
-            raise RuntimeError(L.pk_last_error().decode())
-
-    def measure(path):
-        if path != "exact":
-            idx.prepare_fast(path)
-        ef, recall, sweep = None, 0.0, {}
-        for e in EF_SWEEP:
-            call(path, e)
-            torch.cuda.synchronize()
-            r = datasets.recall_at_k(ids.cpu().numpy(), gt, k)
-            sweep[e] = round(r, 4)
-            if r >= RECALL_TARGET:
-                ef, recall = e, r
-                break
-        if ef is None:
-            ef, recall = EF_SWEEP[-1], sweep[EF_SWEEP[-1]]
-        shape = None
-        if path != "exact":
-            # the launch shape for this batch (results do not depend on it)
-            if args.fast_shape:
-                shape = tuple(int(x) for x in args.fast_shape.split(","))
-                idx.set_fast_params(*shape)
-            else:
-                shape, _ = idx.tune_fast(q_dev, k, ef, args.expand, stream)
-
-        def per_query_counts():
-            cnt = torch.zeros((nq, 6), dtype=torch.int32, device=dev)
-            call(path, ef, counters=cnt)
-            torch.cuda.synchronize()
-            return cnt.double().sum(0).cpu().numpy() / nq
-
-        c = per_query_counts()
-        fetched = c[1] + c[4]
-        if path != "exact":
-            # the tuned walk forgets ids in its small recently-seen table and
-            # fetches some rows again; a 32768-slot table forgets almost
-            # none, so its count is the (near) unique rows the walk needs
-            idx.set_fast_params(shape[0], 15, 1)
-            c = per_query_counts()
-            idx.set_fast_params(*shape)
-        hops_u, dist_u, hops0, dist0 = c[0], c[1], c[3], c[4]
-        # algorithmic bytes per query of the dominant kernel: the rows whose
-        # distances it needs (traversal rows: f16 padded to 32 bytes, fp8 to
-        # 16) and the adjacency lists it reads
-        trav_bytes = {"exact": args.dim * 4, "f16": (args.dim * 2 + 31) // 32 * 32,
-                      "fp8": (args.dim + 15) // 16 * 16}[path]
-        adj_bytes = hops0 * 2 * args.M * 4 + hops_u * args.M * 4
-        bpq = (dist_u + dist0) * trav_bytes + adj_bytes
-        fetched_bpq = fetched * trav_bytes + adj_bytes
+    def timed(path, k, ef, mixed):
+        """K timed steps (after W warm-up steps): total ms and per-step walk ms."""
         for _ in range(args.warmup):
-            call(path, ef)
+            call(path, k, ef, mixed)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -305,160 +370,313 @@ def run_ours(args):
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
                 a.record(stream)
-                call(path, ef)
+                call(path, k, ef, mixed)
                 b.record(stream)
                 b.synchronize()
                 times.append(a.elapsed_time(b))
-                # the dominant kernel alone: the walk (events the library
-                # records around it on this stream), or the exact search
                 kernel_ms.append(idx.fast_timing()[0] if path != "exact" else times[-1])
         torch.cuda.synchronize()
         if path != "exact":
             idx.set_fast_timing(False)
-        total_ms = float(sum(times))
+        total = float(sum(times))
         if world > 1:
-            t = torch.tensor([total_ms], device=dev)
+            t = torch.tensor([total], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
-        # end to end through the C ABI with pinned host buffers
-        for _ in range(args.warmup):
-            host_call(path, ef)
-        e2e = []
-        for _ in range(args.steps):
-            flush.fill_(1)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            host_call(path, ef)
-            e2e.append(time.perf_counter() - t0)
-        e2e_s = float(sum(e2e))
-        if world > 1:
-            t = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        ms = total_ms / args.steps
-        return {"path": path, "ef": ef, "recall": recall, "sweep": sweep, "ms_per_step": ms, "shape": shape,
-                "fetched_bytes_per_query": fetched_bpq, "rows_fetched": fetched,
-                "kernel_ms": float(np.mean(kernel_ms)),
-                "qps": world * nq * args.steps / (total_ms / 1e3), "e2e_qps": world * nq * args.steps / e2e_s,
-                "bytes_per_query": bpq, "dist_evals": dist_u + dist0, "hops0": hops0, "hops_u": hops_u,
-                "clocks": clk.summary()}
+            total = float(t.item())
+        return total, float(np.mean(kernel_ms)), clk.summary()
+
+    def tune(path, k, ef, mixed):
+        if path == "exact":
+            return None
+        if args.fast_shape:
+            shape = tuple(int(x) for x in args.fast_shape.split(","))
+            idx.set_fast_params(*shape)
+            return shape
+        nt = min(nq, 20_000)
+        shape, _ = idx.tune_fast(q_dev[:nt], k, ef, args.expand, stream)
+        return shape
+
+    def counts(path, k, ef, mixed, shape):
+        """Per-query means of the six work counters; for the fast paths with a
+        32768-slot recently-seen table, which forgets almost nothing, so that
+        the rows counted are the (near) distinct rows the walk needs, and with
+        the tuned table (the rows it actually fetches)."""
+        cnt = torch.zeros((nq, 6), dtype=torch.int32, device=dev)
+        call(path, k, ef, mixed, counters=cnt)
+        torch.cuda.synchronize()
+        fetched = cnt.double().mean(0).cpu().numpy()
+        if path == "exact":
+            return fetched, fetched
+        idx.set_fast_params(shape[0], 15, 1)
+        cnt.zero_()
+        call(path, k, ef, mixed, counters=cnt)
+        torch.cuda.synchronize()
+        idx.set_fast_params(*shape)
+        return cnt.double().mean(0).cpu().numpy(), fetched
+
+    elem = {"f16": 2, "f32": 4}[w["dtype"]]
+    trav_bytes = {"exact": w["dim"] * elem, "f16": (w["dim"] * 2 + 31) // 32 * 32,
+                  "fp8": (w["dim"] + 31) // 32 * 32}
+
+    def algorithmic_bytes(path, c):
+        # distinct rows x their value bytes + the adjacency rows read (layer 0
+        # holds 2M slots per node, upper layers M)
+        return (c[1] + c[4]) * trav_bytes[path] + c[3] * 2 * w["M"] * 4 + c[0] * w["M"] * 4
 
     results = {}
     for path in args.paths.split(","):
-        results[path] = measure(path)
-        log(args, f"[{rank}] {path}: ef={results[path]['ef']} recall={results[path]['recall']:.4f} "
-                  f"qps={results[path]['qps']:.0f} e2e={results[path]['e2e_qps']:.0f}")
-    ok = [r for r in results.values() if r["recall"] >= RECALL_TARGET] or list(results.values())
-    best = max(ok, key=lambda r: r["qps"])
+        if path != "exact":
+            idx.prepare_fast(path)
+        r = {"path": path}
+        # the k = 10 recall@10 >= 0.95 point: recall on the sample, QPS on the whole batch
+        sweep, ef10 = {}, None
+        qs = q_dev[:ns]
+        for e in w["sweep"]:
+            call(path, 10, e, False, q=qs, out_i=ids[:ns, :10], out_d=ds[:ns, :10])
+            torch.cuda.synchronize()
+            rc = datasets.recall_at_k(ids[:ns, :10].cpu().numpy(), gt, 10)
+            sweep[e] = round(rc, 4)
+            if rc >= RECALL_TARGET:
+                ef10 = e
+                break
+        if ef10 is None:
+            ef10 = w["sweep"][-1]
+        shape10 = tune(path, 10, ef10, False)
+        tot10, kms10, clk10 = timed(path, 10, ef10, False)
+        r["k10"] = {"ef": ef10, "recall_at_10": sweep[ef10], "ef_sweep_recall": sweep, "launch_shape": shape10,
+                    "qps": world * nq * args.steps / (tot10 / 1e3), "ms_per_step": tot10 / args.steps,
+                    "kernel_ms": kms10, "clocks": clk10}
+        if w["mixed"]:
+            efmax = int(efq.max())
+            shape = tune(path, 100, 384, False)
+            tot, kms, clk = timed(path, kmax, efmax, True)
+            call(path, kmax, efmax, True)
+            torch.cuda.synchronize()
+            rec = recall_mixed(ids[:ns].cpu().numpy(), gt, kq[:ns])
+            c_alg, c_fetch = counts(path, kmax, efmax, True, shape)
+            r["mixed"] = {"recall_at_k": rec, "launch_shape": shape, "qps": world * nq * args.steps / (tot / 1e3),
+                          "ms_per_step": tot / args.steps, "kernel_ms": kms, "clocks": clk,
+                          "bytes_per_query": algorithmic_bytes(path, c_alg), "counters": c_alg.tolist(),
+                          "rows_fetched": float(c_fetch[1] + c_fetch[4])}
+        else:
+            c_alg, c_fetch = counts(path, 10, ef10, False, shape10)
+            r["k10"].update(bytes_per_query=algorithmic_bytes(path, c_alg), counters=c_alg.tolist(),
+                            rows_fetched=float(c_fetch[1] + c_fetch[4]))
+        results[path] = r
+        log(args, f"[{rank}] {path}: " + json.dumps({x: {kk: v for kk, v in r[x].items() if kk != 'clocks'}
+                                                     for x in ("k10", "mixed") if x in r}))
+
+    head = "mixed" if w["mixed"] else "k10"
+    ok = [r for r in results.values() if w["mixed"] or r["k10"]["recall_at_10"] >= RECALL_TARGET]
+    best = max(ok or list(results.values()), key=lambda r: r[head]["qps"])
+    bp = best["path"]
+    bh = best[head]
+
+    # end to end through the C ABI with pinned host buffers
+    qh = torch.from_numpy(queries).pin_memory()
+    kh = torch.from_numpy(kq).pin_memory()
+    eh = torch.from_numpy(efq if efq is not None else np.full(nq, bh.get("ef", best["k10"]["ef"]), np.int32))
+    eh = eh.pin_memory()
+    stride = kmax if w["mixed"] else 10
+    ih = torch.empty((nq, stride), dtype=torch.int32).pin_memory()
+    dh = torch.empty((nq, stride), dtype=torch.float32).pin_memory()
+    ef_u = best["k10"]["ef"]
+    if bp != "exact":
+        idx.set_fast_params(*(bh["launch_shape"]))
+
+    def host_call():
+        qp, ip_, dp = (ctypes.c_void_p(t.data_ptr()) for t in (qh, ih, dh))
+        if w["mixed"] and bp != "exact":
+            rc = L.pk_index_search_fast_host_var(idx._h, qp, nq, ctypes.c_void_p(kh.data_ptr()),
+                                                 ctypes.c_void_p(eh.data_ptr()), stride, ip_, dp, args.expand)
+        elif w["mixed"]:
+            rc = L.pk_index_search_var(idx._h, qp, nq, ctypes.c_void_p(kh.data_ptr()), ctypes.c_void_p(eh.data_ptr()),
+                                       stride, ip_, dp)
+        elif bp == "exact":
+            rc = L.pk_index_search(idx._h, qp, nq, stride, ef_u, ip_, dp)
+        else:
+            rc = L.pk_index_search_fast_host(idx._h, qp, nq, stride, ef_u, ip_, dp, args.expand)
+        if rc != 0:
+            raise RuntimeError(L.pk_last_error().decode())
+
+    for _ in range(args.warmup):
+        host_call()
+    e2e = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        host_call()
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = float(sum(e2e))
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_qps = world * nq * args.steps / e2e_s
+
     peak, peak_kind = measured_peaks()
-    kernel = "search_exact_kernel" if best["path"] == "exact" else "walk_kernel"
-    achieved = best["bytes_per_query"] * nq / (best["kernel_ms"] / 1e3) / 1e9
-    tr = ncu_traffic_per_query(kernel)
-    traffic = None
-    if (tr and tr.get("workload") == "1Mx96" and tr.get("path") == best["path"] and tr.get("ef") == best["ef"]
-            and "dram_bytes_per_query" in tr):
-        traffic = round(tr["dram_bytes_per_query"] * nq)
+    kernel = "search_exact_kernel" if bp == "exact" else "walk_kernel"
+    rf = best["mixed"] if w["mixed"] else best["k10"]
+    achieved = rf["bytes_per_query"] * nq / (rf["kernel_ms"] / 1e3) / 1e9
+    tr = profiled_traffic(args.workload, bp)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        with tempfile.TemporaryDirectory() as td:
-            gp = os.path.join(td, "g.pkg")
-            idx.save(gp)
-            cpu = cpu_baseline(args, gp, queries, results.get("exact", best)["ef"])
+        import oracle
+        if oracle.ref_available():
+            gp = saved or graph_file(args, w)
+            tmpdir = None
+            if not gp or not os.path.exists(gp):
+                tmpdir = tempfile.mkdtemp(prefix="pk_bench_")
+                gp = os.path.join(tmpdir, "g.pkg")
+                idx.save(gp)
+            ns_cpu = min(args.cpu_sample, nq)
+            if w["mixed"]:
+                secs, threads = cpu_reference(gp, queries[:ns_cpu], kmax, int(efq.max()), kq[:ns_cpu],
+                                              efq[:ns_cpu], 3)
+                what = f"{ns_cpu} queries of the mixed batch with their own k and ef"
+            else:
+                secs, threads = cpu_reference(gp, queries[:ns_cpu], 10, best["k10"]["ef"], None, None, 3)
+                what = f"{ns_cpu} of the {nq} queries at ef={best['k10']['ef']}"
+            cpu = {"value": round(ns_cpu / statistics.median(secs), 1), "unit": "queries/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": what + ", same graph file, median of 3 batch runs (steady clock around the batch)"}
+            if tmpdir:
+                os.remove(gp)
+                os.rmdir(tmpdir)
 
     if rank == 0:
         plain = results.get("exact")
+
+        def path_line(r):
+            out = {}
+            for key in ("mixed", "k10"):
+                if key not in r:
+                    continue
+                x = r[key]
+                out[key] = {kk: (round(v, 4) if isinstance(v, float) else v) for kk, v in x.items()
+                            if kk not in ("clocks", "counters")}
+                if plain and key in plain:
+                    out[key]["speedup_vs_plain_fp32"] = round(x["qps"] / plain[key]["qps"], 3)
+            return out
+
+        launches = 1 if bp == "exact" else (3 + (8 if w["mixed"] else 1))
         line = {
-            "metric": METRIC_NAME,
-            "value": round(best["qps"], 1),
+            "metric": metric_name(w),
+            "value": round(bh["qps"], 1),
             "unit": "queries/s",
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": round(best["ms_per_step"], 4),
+            "ms_per_step": round(bh["ms_per_step"], 4),
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32",
-            "data": "synthetic (seeded Gaussian mixture, unit rows; stands in for the public datasets)",
-            "config": {"workload": f"{args.n // 1000}k x {args.dim} f32 IP, M={args.M}, efC={args.efc}, "
-                                   f"{nq} queries per GPU, k={k}",
-                       "n": args.n, "dim": args.dim, "metric": "ip", "M": args.M, "ef_construction": args.efc,
-                       "queries_per_gpu": nq, "k": k, "path": best["path"], "ef": best["ef"],
-                       "recall_at_10": round(best["recall"], 4),
-                       "paths": {p: {"ef": r["ef"], "recall_at_10": round(r["recall"], 4), "qps": round(r["qps"], 1),
-                                     "e2e_qps": round(r["e2e_qps"], 1), "ms_per_step": round(r["ms_per_step"], 4),
-                                     "kernel_ms": round(r["kernel_ms"], 4), "launch_shape": r["shape"],
-                                     "ef_sweep_recall": r["sweep"]} for p, r in results.items()},
-                       "speedup_vs_plain_fp32": round(best["qps"] / plain["qps"], 3) if plain else None,
-                       "l2": "flushed between steps (256 MiB write); index 640 MB > L2",
-                       "build_s": round(build_s, 2), "parallelism": f"replicas x{world}"},
-            "e2e": {"value": round(best["e2e_qps"], 1), "unit": "queries/s",
-                    "h2d_bytes_per_step": nq * args.dim * 4, "d2h_bytes_per_step": nq * k * 8},
-            # exact: the search kernel; fast: query conversion, walk, re-rank
-            "gpu_launches": args.steps * (1 if best["path"] == "exact" else 3),
+            "dtype": "f16" if w["dtype"] == "f16" else "f32",
+            "data": "synthetic (seeded Gaussian mixture; stands in for the public datasets)",
+            "config": {"workload": workload_name(w), "n": w["n"], "dim": w["dim"], "metric": w["metric"],
+                       "M": w["M"], "ef_construction": w["efc"], "queries_per_gpu": nq, "path": bp,
+                       "recall": round(bh.get("recall_at_k", bh.get("recall_at_10", 0.0)), 4),
+                       "recall_sample": f"first {ns} queries, float64 exact ground truth",
+                       "paths": {p: path_line(r) for p, r in results.items()},
+                       "speedup_vs_plain_fp32": (round(bh["qps"] / plain[head]["qps"], 3) if plain else None),
+                       "l2": "index 10.7 GB >> L2; 256 MiB written between steps" if w["mixed"] else
+                             "index > L2; 256 MiB written between steps",
+                       "graph": ("GPU build " + (f"{build_s:.1f} s" if build_s is not None else
+                                                 "loaded from the bench's graph cache")),
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s",
+                    "h2d_bytes_per_step": int(queries.nbytes + (kq.nbytes + efq.nbytes if w["mixed"] else 0)),
+                    "d2h_bytes_per_step": int(nq * stride * 8)},
+            "gpu_launches": args.steps * launches,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": kernel, "kernel_ms": round(best["kernel_ms"], 4),
-                         "bytes_per_query": round(best["bytes_per_query"], 1),
-                         "fetched_bytes_per_query": round(best["fetched_bytes_per_query"], 1),
-                         "per_query": {"dist_evals": round(best["dist_evals"], 1), "hops_l0": round(best["hops0"], 1),
-                                       "hops_upper": round(best["hops_u"], 1),
-                                       "rows_fetched": round(best["rows_fetched"], 1)}},
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": (round(tr["dram_bytes_per_query"] * nq) if tr else None),
+                         "traffic_source": (tr["source"] if tr else None),
+                         "kernel": kernel, "kernel_ms": round(rf["kernel_ms"], 4),
+                         "bytes_per_query": round(rf["bytes_per_query"], 1),
+                         "rows_fetched_per_query": round(rf["rows_fetched"], 1),
+                         "per_query": dict(zip(["hops_upper", "dists_upper", "nbrs_upper", "hops_l0", "dists_l0",
+                                                "nbrs_l0"], [round(v, 1) for v in rf["counters"]]))},
             "cpu_baseline": cpu,
-            "clocks": best["clocks"],
+            "clocks": bh["clocks"],
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------- reference --
+
 def run_reference(args):
-    """The reference's own Build and AnnSearch on the host cores (rank 0 only)."""
+    """The reference's own AnnSearch (oracle/_ref/pk_ref) on the host cores,
+    rank 0 only, on a sample of the same batch and the same GPU-built graph."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import oracle
-    from pickle_b200 import datasets
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pk_ref was not built"}))
         return
-    base, queries = make_data(args, 0)
+    import torch
+
+    from pickle_b200 import datasets
+    from pickle_b200.groundtruth import gpu_knn
+    w = workload(args)
+    base, queries = make_data(w, args.seed, 0)
+    idx, build_s, saved = build_or_load(args, w, base, 0)
+    gp = saved or graph_file(args, w)
+    tmpdir = None
+    if not gp or not os.path.exists(gp):
+        tmpdir = tempfile.mkdtemp(prefix="pk_bench_ref_")
+        gp = os.path.join(tmpdir, "g.pkg")
+        idx.save(gp)
+    idx.close()
+    ns = min(args.cpu_sample, len(queries))
+    kq, efq = per_query_k_ef(w, len(queries), args.seed)
+    sample = queries[:ns]
+    gt = gpu_knn(base, sample, 100 if w["mixed"] else 10, w["metric"], torch.device("cuda"))
+    del base
     threads = os.cpu_count() or 1
-    with tempfile.TemporaryDirectory() as td:
-        gp = os.path.join(td, "ref.pkg")
-        t0 = time.time()
-        binfo = oracle.ref_build(base, "ip", args.M, args.efc, gp, threads=threads)
-        build_s = time.time() - t0
-        sample = queries[: args.cpu_sample]
-        gt, _ = datasets.exact_knn(base, sample, args.k, "ip")
-        ef, recall, sweep = EF_SWEEP[-1], None, {}
-        for e in EF_SWEEP:
-            ri, _, _ = oracle.ref_search(gp, sample, args.k, e, threads=threads)
-            r = datasets.recall_at_k(ri, gt, args.k)
-            sweep[e] = round(r, 4)
-            if r >= RECALL_TARGET:
-                ef, recall = e, r
-                break
-        steps = []
-        for _ in range(args.warmup):
-            oracle.ref_search(gp, sample, args.k, ef, threads=threads, want_results=False)
-        for _ in range(args.steps):
-            _, _, info = oracle.ref_search(gp, sample, args.k, ef, threads=threads, want_results=False)
-            steps.append(info["median_s"])
-    total = sum(steps)
-    value = len(sample) * args.steps / total
+    # the k = 10 recall@10 >= 0.95 point of the reference on this graph
+    sweep, ef10 = {}, w["sweep"][-1]
+    for e in w["sweep"]:
+        ri, _, _ = oracle.ref_search(gp, sample, 10, e, threads=threads)
+        r = datasets.recall_at_k(ri, gt, 10)
+        sweep[e] = round(r, 4)
+        if r >= RECALL_TARGET:
+            ef10 = e
+            break
+    if w["mixed"]:
+        ri, _, info = oracle.ref_search(gp, sample, int(kq.max()), int(efq.max()), threads=threads,
+                                        repeat=args.warmup + args.steps, k_per_query=kq[:ns],
+                                        ef_per_query=efq[:ns])
+        recall = recall_mixed(ri, gt, kq[:ns])
+    else:
+        ri, _, info = oracle.ref_search(gp, sample, 10, ef10, threads=threads, repeat=args.warmup + args.steps)
+        recall = datasets.recall_at_k(ri, gt, 10)
+    secs = info["all_s"][args.warmup:]
+    total = float(sum(secs))
+    value = ns * args.steps / total
+    _, _, i10 = oracle.ref_search(gp, sample, 10, ef10, threads=threads, repeat=3, want_results=False)
+    if tmpdir:
+        os.remove(gp)
+        os.rmdir(tmpdir)
     line = {
-        "metric": METRIC_NAME, "value": round(value, 1), "unit": "queries/s", "n_gpus": 0, "steps": args.steps,
+        "metric": metric_name(w), "value": round(value, 1), "unit": "queries/s", "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
-        "data": "synthetic (seeded Gaussian mixture, unit rows)",
-        "config": {"workload": f"{args.n // 1000}k x {args.dim} f32 IP, M={args.M}, efC={args.efc}, k={args.k}",
-                   "ef": ef, "recall_at_10": recall, "ef_sweep_recall": sweep, "build_s": round(build_s, 1),
-                   "queries_per_step": len(sample)},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16" if w["dtype"] == "f16" else "f32",
+        "impl": "reference", "data": "synthetic (seeded Gaussian mixture)",
+        "config": {"workload": workload_name(w), "queries_per_step": ns,
+                   "recall": round(recall, 4), "k10": {"ef": ef10, "recall_at_10": sweep[ef10],
+                                                       "ef_sweep_recall": sweep, "qps": round(i10["qps"], 1)},
+                   "graph": "the GPU-built graph (a reference Build of this size takes hours on the host cores), "
+                            + ("built here" if build_s is not None else "from the bench's graph cache")},
         "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads, "kind": "reference",
-                         "sample": f"{len(sample)} queries per step, batch AnnSearch, graph built by the "
-                                   f"reference's own Build on {threads} threads"},
+                         "sample": f"{ns} queries per step (the first {ns} of the batch"
+                                   + (", each with its own k and ef)" if w["mixed"] else ")")
+                                   + ", the reference's batch AnnSearch loop on all host threads"},
         "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -466,6 +684,8 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_distributed(args))
     if args.impl == "reference":
         run_reference(args)
     else:

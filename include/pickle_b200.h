@@ -100,6 +100,14 @@ int pk_index_add(pk_index *h, const void *rows, int64_t n, const int32_t *ext_id
 int pk_index_search(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
                     float *out_dists);
 
+/* pk_index_search with a k and an ef per query: the reference's batch loop
+ * (include/hnsw.hpp:528-541) over its single-query AnnSearch (:509-525) with
+ * each query's own values.  Host buffers: queries nq*dim, out_ids / out_dists
+ * nq*out_stride (out_stride >= the largest k; row i holds k_per_query[i]
+ * results, then -1 / FLT_MAX).  Synchronous. */
+int pk_index_search_var(pk_index *h, const void *queries, int64_t nq, const int32_t *k_per_query,
+                        const int32_t *ef_per_query, int32_t out_stride, int32_t *out_ids, float *out_dists);
+
 /* Device-resident batch search, asynchronous on `stream` (a cudaStream_t,
  * NULL = legacy default stream).  All pointers are device pointers.
  *  k_per_query / ef_per_query: nq values each, or NULL to use k / ef for all.
@@ -143,6 +151,16 @@ int pk_index_search_fast(pk_index *h, const void *queries, int64_t nq, int32_t k
  * walk did not complete within its bound (the results are then -1). */
 int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t *out_ids,
                               float *out_dists, int32_t expand);
+
+/* pk_index_search_fast with host buffers and a k and an ef per query (the
+ * reference's batch AnnSearch takes one k and one ef for the whole batch,
+ * include/hnsw.hpp:528-541; its single-query AnnSearch, :509-525, takes them
+ * per call): queries nq*dim in, out_ids / out_dists nq*out_stride out
+ * (out_stride >= the largest k; row i holds k_per_query[i] results, then
+ * -1 / FLT_MAX).  Synchronous; PK_ERR_TIMEOUT as pk_index_search_fast_host. */
+int pk_index_search_fast_host_var(pk_index *h, const void *queries, int64_t nq, const int32_t *k_per_query,
+                                  const int32_t *ef_per_query, int32_t out_stride, int32_t *out_ids,
+                                  float *out_dists, int32_t expand);
 
 /* Launch shape of pk_index_search_fast's walk (0 keeps the default):
  * rows_per_batch = vector rows fetched per round trip (1..256; default

@@ -60,8 +60,30 @@ def lib() -> ctypes.CDLL:
         L.ora_distance.argtypes = [I32, I32, VP, VP, I64]
         L.ora_cumulative_probability.argtypes = [I64, VP, I32]
         L.ora_layer.argtypes = [P, I32] + [VP] * 7
+        L.ora_set_float_order.argtypes = [I32]
+        L.ora_search_fork.argtypes = [P, VP, I64, I32, I32, I32, I32, VP, VP, VP, I32, VP, VP, VP, VP, I64, VP]
         _lib = L
     return _lib
+
+
+# Float summation orders (pk_oracle.h): the reference's source order, the
+# device library's order, or distances looked up in a table.
+ORDER_SOURCE, ORDER_DEVICE, ORDER_TABLE = 0, 1, 2
+
+
+class float_order:
+    """Context manager: float32 / float16 distances of the restatement in the
+    given order (ORDER_SOURCE or ORDER_DEVICE) while it is active."""
+
+    def __init__(self, order: int):
+        self.order = order
+
+    def __enter__(self):
+        lib().ora_set_float_order(self.order)
+        return self
+
+    def __exit__(self, *exc):
+        lib().ora_set_float_order(ORDER_SOURCE)
 
 
 def _ptr(a: np.ndarray):
@@ -127,6 +149,43 @@ class OraGraph:
         if rc != 0:
             raise RuntimeError(f"oracle search failed: {rc}")
         return (ids, dists, cnt) if counters else (ids, dists)
+
+    def search_fork(self, queries: np.ndarray, k: int, ef: int, order_a: int, order_b: int, table=None,
+                    threads: int = 0, touched_cap: int = 0):
+        """AnnSearch replayed with two sets of float distances (ora_search_fork).
+
+        order_a drives the search; order_b (ORDER_SOURCE, ORDER_DEVICE, or
+        ORDER_TABLE with table = (offsets[nq+1] int64, keys int32, values
+        float32), keys sorted per query) is compared at every decision.
+        Returns (ids, dists, fork, touched): fork is nq x 6 float64 =
+        {forked, where, a_x, a_y, b_x, b_y} for the first comparison whose
+        outcome differs (where: 1 SlideLayer, 2 early exit, 3 admission,
+        4 heap order, 5 table miss); touched (with touched_cap > 0) is a list
+        per query of the row keys (external id, -1 = zero row) whose
+        distances the order_a search evaluated."""
+        q = np.ascontiguousarray(queries)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.int32)
+        dists = np.empty((nq, k), np.float32)
+        fork = np.zeros((nq, 6), np.float64)
+        toff = tkey = tval = None
+        if order_b == ORDER_TABLE:
+            toff, tkey, tval = (np.ascontiguousarray(table[0], np.int64), np.ascontiguousarray(table[1], np.int32),
+                                np.ascontiguousarray(table[2], np.float32))
+        touched = np.empty((nq, max(touched_cap, 1)), np.int32) if touched_cap else None
+        tn = np.zeros(nq, np.int64)
+        rc = lib().ora_search_fork(self.h, _ptr(q), nq, k, ef, order_a, order_b,
+                                   _ptr(toff) if toff is not None else None, _ptr(tkey) if tkey is not None else None,
+                                   _ptr(tval) if tval is not None else None, threads, _ptr(ids), _ptr(dists),
+                                   _ptr(fork), _ptr(touched) if touched is not None else None, touched_cap, _ptr(tn))
+        if rc != 0:
+            raise RuntimeError(f"oracle fork search failed: {rc}")
+        lists = None
+        if touched is not None:
+            if (tn > touched_cap).any():
+                raise ValueError(f"touched_cap {touched_cap} < {int(tn.max())}")
+            lists = [touched[i, :tn[i]].copy() for i in range(nq)]
+        return ids, dists, fork, lists
 
     def layer(self, level: int) -> dict:
         n, cap = ctypes.c_int64(), ctypes.c_int64()
@@ -196,12 +255,20 @@ def ref_build(data: np.ndarray, metric: str, M: int, efc: int, out_path: str, th
 
 
 def ref_search(graph_path: str, queries: np.ndarray, k: int, ef: int, threads: int = 0, repeat: int = 1,
-               metrics: bool = False, dynamic: bool = False, want_results: bool = True):
-    """Batch AnnSearch with the reference's code on a v2 graph file."""
+               metrics: bool = False, dynamic: bool = False, want_results: bool = True, k_per_query=None,
+               ef_per_query=None):
+    """Batch AnnSearch with the reference's code on a v2 graph file.  With
+    k_per_query / ef_per_query, each query runs the single-query AnnSearch
+    with its own values (k is then the width of the returned rows)."""
     with tempfile.TemporaryDirectory() as td:
         qp = os.path.join(td, "q.npy")
         np.save(qp, np.ascontiguousarray(queries))
         args = ["search", "--graph", graph_path, "--queries", qp, "--k", k, "--ef", ef, "--repeat", repeat]
+        if k_per_query is not None:
+            kp, ep = os.path.join(td, "kq.npy"), os.path.join(td, "efq.npy")
+            np.save(kp, np.ascontiguousarray(k_per_query, np.int32))
+            np.save(ep, np.ascontiguousarray(ef_per_query, np.int32))
+            args += ["--kq", kp, "--efq", ep]
         if threads:
             args += ["--threads", threads]
         if metrics:

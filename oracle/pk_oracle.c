@@ -120,15 +120,78 @@ static float dist_i8(const int8_t *a, const int8_t *b, int64_t dim, int ip) {
     return ip ? -(float)s : (float)s;
 }
 
-float ora_distance(int dtype, int metric, const void *a, const void *b, int64_t dim) {
+/* The summation order of the device library's float distances
+ * (pickle_b200/csrc/pk_warp.cuh, Acc / dist_rows / dist_rows_staged; lane
+ * layout of lane_config in pk_internal.h): the row, zero padded to C 16-byte
+ * chunks, is split over a group of G lanes (G the power of two >= C/4, from 2
+ * to 32), lane g accumulating chunks g, g + G, ... in element order with fused
+ * multiply-adds; the G partial sums are then combined by a butterfly
+ * (partial[g] += partial[g ^ off] for off = G/2, ..., 1) and lane 0's sum is
+ * the distance.  Restated here so that the oracle can replay a search with
+ * the device's own float distances. */
+static float dist_device_order(int dtype, const void *a, const void *b, int64_t dim, int ip) {
+    const int64_t esz = dtype == 2 ? 4 : 2, per = 16 / esz;
+    const int C = (int)((dim * esz + 15) / 16);
+    const int want = (C + 3) / 4;
+    int G = 2;
+    while (G < want && G < 32) G *= 2;
+    const int K = (C + G - 1) / G;
+    float part[32], nxt[32];
+    for (int g = 0; g < G; g++) {
+        float acc = 0.0f;
+        for (int k = 0; k < K; k++) {
+            const int c = g + k * G;
+            if (c >= C) continue;
+            for (int64_t e = 0; e < per; e++) {
+                const int64_t i = (int64_t)c * per + e;
+                float x = 0.0f, y = 0.0f;
+                if (i < dim) {
+                    if (dtype == 2) {
+                        x = ((const float *)a)[i];
+                        y = ((const float *)b)[i];
+                    } else {
+                        x = half_to_float(((const uint16_t *)a)[i]);
+                        y = half_to_float(((const uint16_t *)b)[i]);
+                    }
+                }
+                if (ip) {
+                    acc = fmaf(x, y, acc);
+                } else {
+                    const float d = x - y;
+                    acc = fmaf(d, d, acc);
+                }
+            }
+        }
+        part[g] = acc;
+    }
+    for (int off = G >> 1; off > 0; off >>= 1) {
+        for (int g = 0; g < G; g++) nxt[g] = part[g] + part[g ^ off];
+        for (int g = 0; g < G; g++) part[g] = nxt[g];
+    }
+    return ip ? -part[0] : part[0];
+}
+
+static int g_float_order = ORA_ORDER_SOURCE;
+
+void ora_set_float_order(int order) { g_float_order = order == ORA_ORDER_DEVICE ? ORA_ORDER_DEVICE : ORA_ORDER_SOURCE; }
+
+static float distance_in_order(int order, int dtype, int metric, const void *a, const void *b, int64_t dim) {
     int ip = metric == 2;
     switch (dtype) {
         case 0: return dist_u8((const uint8_t *)a, (const uint8_t *)b, dim, ip);
         case 1: return dist_i8((const int8_t *)a, (const int8_t *)b, dim, ip);
-        case 2: return dist_float((const float *)a, (const float *)b, dim, ip);
-        case 3: return dist_half((const uint16_t *)a, (const uint16_t *)b, dim, ip);
+        case 2:
+            return order == ORA_ORDER_DEVICE ? dist_device_order(2, a, b, dim, ip)
+                                             : dist_float((const float *)a, (const float *)b, dim, ip);
+        case 3:
+            return order == ORA_ORDER_DEVICE ? dist_device_order(3, a, b, dim, ip)
+                                             : dist_half((const uint16_t *)a, (const uint16_t *)b, dim, ip);
         default: return NAN;
     }
+}
+
+float ora_distance(int dtype, int metric, const void *a, const void *b, int64_t dim) {
+    return distance_in_order(g_float_order, dtype, metric, a, b, dim);
 }
 
 /* ------------------------------------------------------------------ */
@@ -459,6 +522,274 @@ int ora_search(const ora_graph *g, const void *queries, int64_t nq, int k, int e
             if (cnt) memset(cnt, 0, 6 * sizeof(int64_t));
             ann_search(g, &s, (const char *)queries + i * qb, k, ef, ids + i * k, dists + i * k, cnt);
         }
+        scratch_free(&s);
+    }
+    return g->err ? -2 : 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* fork detector: AnnSearch replayed with two sets of float distances  */
+/* ------------------------------------------------------------------ */
+/* The same steps as slide_layer / search_layer / ann_search above, on entries
+ * that carry a distance in the driving order (a) and in the compared order
+ * (b).  Every decision follows a; each comparison of two distances is also
+ * made with b, and the first one whose outcome differs is recorded. */
+
+typedef struct {
+    float a, b;
+    int32_t id;
+} dent;
+
+typedef struct {
+    dent *v;
+    int64_t len, cap;
+    int maxfirst;
+} dheap;
+
+typedef struct {
+    const ora_graph *g;
+    int order_a, order_b;
+    const int32_t *tkey;
+    const float *tval;
+    int64_t tn;
+    double *fork;
+    int32_t *touched;
+    int64_t tcap, tcount;
+} fctx;
+
+static void fk_note(fctx *c, int where, float xa, float ya, float xb, float yb) {
+    if (c->fork[0] != 0.0) return;
+    c->fork[0] = 1.0;
+    c->fork[1] = where;
+    c->fork[2] = xa;
+    c->fork[3] = ya;
+    c->fork[4] = xb;
+    c->fork[5] = yb;
+}
+
+/* x < y in order a; a different outcome in order b is the fork. */
+static inline int fk_lt(fctx *c, int where, float xa, float ya, float xb, float yb) {
+    const int ra = xa < ya, rb = xb < yb;
+    if (ra != rb) fk_note(c, where, xa, ya, xb, yb);
+    return ra;
+}
+
+/* The heaps' comparator (include/queue.hpp:30-40): MaxFirst l < r, MinFirst l > r. */
+static inline int dh_cmp(fctx *c, const dheap *h, dent l, dent r) {
+    return h->maxfirst ? fk_lt(c, 4, l.a, r.a, l.b, r.b) : fk_lt(c, 4, r.a, l.a, r.b, l.b);
+}
+
+static void dh_init(dheap *h, int maxfirst) {
+    h->cap = 512;
+    h->len = 0;
+    h->maxfirst = maxfirst;
+    h->v = (dent *)malloc(sizeof(dent) * h->cap);
+}
+
+/* hpush / hpop above, step for step. */
+static void dh_push(fctx *c, dheap *h, dent e) {
+    if (h->len >= h->cap) {
+        h->cap *= 8;
+        h->v = (dent *)realloc(h->v, sizeof(dent) * h->cap);
+    }
+    int64_t i = h->len++;
+    while (i > 0) {
+        int64_t p = (i - 1) / 2;
+        if (!dh_cmp(c, h, h->v[p], e)) break;
+        h->v[i] = h->v[p];
+        i = p;
+    }
+    h->v[i] = e;
+}
+
+static void dh_pop(fctx *c, dheap *h) {
+    h->v[0] = h->v[h->len - 1];
+    h->len--;
+    if (h->len == 0) return;
+    int64_t i = 0;
+    for (;;) {
+        int64_t l = 2 * i + 1, r = 2 * i + 2, best = i;
+        if (l < h->len && dh_cmp(c, h, h->v[best], h->v[l])) best = l;
+        if (r < h->len && dh_cmp(c, h, h->v[best], h->v[r])) best = r;
+        if (best == i) return;
+        dent t = h->v[i];
+        h->v[i] = h->v[best];
+        h->v[best] = t;
+        i = best;
+    }
+}
+
+static dent dh_extract(fctx *c, dheap *h) {
+    dent e = h->v[0];
+    dh_pop(c, h);
+    return e;
+}
+
+/* The row a layer's node is compared with: its external id, or -1 for the
+ * zero row (see get_data). */
+static inline int32_t row_key(const ora_graph *g, int level, int32_t vid) {
+    int32_t e = g->L[level].ext[vid];
+    return (e < 0 || !g->L[level].hasvec[vid]) ? -1 : e;
+}
+
+static dent fk_dist(fctx *c, const void *q, int level, int32_t vid) {
+    const ora_graph *g = c->g;
+    const void *row = get_data(g, level, vid);
+    const int32_t key = row_key(g, level, vid);
+    if (c->touched && c->tcount < c->tcap) c->touched[c->tcount] = key;
+    c->tcount++;
+    dent e;
+    e.id = vid;
+    e.a = distance_in_order(c->order_a, g->dtype, g->metric, q, row, g->dim);
+    if (c->order_b != ORA_ORDER_TABLE) {
+        e.b = distance_in_order(c->order_b, g->dtype, g->metric, q, row, g->dim);
+        return e;
+    }
+    int64_t lo = 0, hi = c->tn;
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (c->tkey[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    if (lo < c->tn && c->tkey[lo] == key) {
+        e.b = c->tval[lo];
+    } else {
+        e.b = e.a;
+        fk_note(c, 5, e.a, e.a, NAN, NAN);
+    }
+    return e;
+}
+
+static int32_t fk_slide(fctx *c, scratch *s, int32_t enter, int level, const void *q) {
+    const ora_graph *g = c->g;
+    const olayer *L = &g->L[level];
+    vs_begin(&s->vis, L->lcap);
+    int32_t best = enter;
+    dent cd = fk_dist(c, q, level, enter);
+    vs_mark(&s->vis, enter);
+    int updated;
+    do {
+        updated = 0;
+        int32_t cur = best;
+        int64_t deg = L->deg[cur];
+        const int32_t *adj = L->adj + (int64_t)cur * L->cap;
+        for (int64_t i = 0; i < deg; i++) {
+            int32_t v = adj[i];
+            if (bad_id(g, L, v)) continue;
+            if (!vs_test(&s->vis, v)) {
+                dent d = fk_dist(c, q, level, v);
+                if (fk_lt(c, 1, d.a, cd.a, d.b, cd.b)) {
+                    best = v;
+                    cd = d;
+                    updated = 1;
+                }
+                vs_mark(&s->vis, v);
+            }
+        }
+    } while (updated);
+    return best;
+}
+
+static void fk_search_layer(fctx *c, scratch *s, dheap *cand, dheap *nn, int32_t enter, int level, int ef,
+                            const void *q) {
+    const ora_graph *g = c->g;
+    const olayer *L = &g->L[level];
+    vs_begin(&s->vis, L->lcap);
+    cand->len = 0;
+    nn->len = 0;
+    dent e = fk_dist(c, q, level, enter);
+    dh_push(c, nn, e);
+    dh_push(c, cand, e);
+    vs_mark(&s->vis, enter);
+    while (cand->len > 0) {
+        dent x = dh_extract(c, cand);
+        const dent t = nn->v[0];
+        if (fk_lt(c, 2, t.a, x.a, t.b, x.b)) break; /* x.d > top.d */
+        int64_t deg = L->deg[x.id];
+        const int32_t *adj = L->adj + (int64_t)x.id * L->cap;
+        for (int64_t i = 0; i < deg; i++) {
+            int32_t v = adj[i];
+            if (bad_id(g, L, v)) continue;
+            if (!vs_test(&s->vis, v)) {
+                vs_mark(&s->vis, v);
+                dent d = fk_dist(c, q, level, v);
+                int admit = nn->len < ef;
+                if (!admit) {
+                    const dent w = nn->v[0];
+                    admit = fk_lt(c, 3, d.a, w.a, d.b, w.b); /* top.d > d */
+                }
+                if (admit) {
+                    dh_push(c, nn, d);
+                    dh_push(c, cand, d);
+                    if (nn->len > ef) dh_pop(c, nn);
+                }
+            }
+        }
+    }
+}
+
+int ora_search_fork(const ora_graph *g, const void *queries, int64_t nq, int k, int ef, int order_a, int order_b,
+                    const int64_t *tb_off, const int32_t *tb_key, const float *tb_val, int nthreads, int32_t *ids,
+                    float *dists, double *fork, int32_t *touched, int64_t touched_cap, int64_t *touched_n) {
+    if (!g || k <= 0 || ef <= 0 || nq < 0 || g->nlayers == 0 || g->L[0].n == 0) return -1;
+    if (order_a == ORA_ORDER_TABLE) return -1;
+    if (order_b == ORA_ORDER_TABLE && (!tb_off || !tb_key || !tb_val)) return -1;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    size_t qb = (size_t)g->dim * g->esz;
+#pragma omp parallel
+    {
+        scratch s;
+        scratch_init(&s);
+        dheap cand, nn;
+        dh_init(&cand, 0);
+        dh_init(&nn, 1);
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t i = 0; i < nq; i++) {
+            const void *q = (const char *)queries + i * qb;
+            fctx c;
+            memset(&c, 0, sizeof(c));
+            c.g = g;
+            c.order_a = order_a;
+            c.order_b = order_b;
+            c.fork = fork + 6 * i;
+            memset(c.fork, 0, 6 * sizeof(double));
+            if (order_b == ORA_ORDER_TABLE) {
+                c.tkey = tb_key + tb_off[i];
+                c.tval = tb_val + tb_off[i];
+                c.tn = tb_off[i + 1] - tb_off[i];
+            }
+            if (touched) {
+                c.touched = touched + i * touched_cap;
+                c.tcap = touched_cap;
+            }
+            /* ann_search */
+            int32_t enter_ext = -1, enter_in = -1;
+            for (int level = g->enter_level; level >= 1; level--) {
+                enter_in = ent_in(g, enter_ext, level);
+                enter_in = fk_slide(&c, &s, enter_in, level, q);
+                enter_ext = g->L[level].ext[enter_in];
+            }
+            enter_in = ent_in(g, enter_ext, 0);
+            fk_search_layer(&c, &s, &cand, &nn, enter_in, 0, ef, q);
+            int64_t kk = k < nn.len ? k : nn.len;
+            while (nn.len > kk) dh_pop(&c, &nn);
+            int32_t *oi = ids + i * k;
+            float *od = dists + i * k;
+            for (int64_t j = 0; j < k; j++) {
+                oi[j] = -1;
+                od[j] = FLT_MAX;
+            }
+            for (int64_t j = 0; j < kk; j++) {
+                dent e = dh_extract(&c, &nn);
+                oi[kk - j - 1] = g->L[0].ext[e.id];
+                od[kk - j - 1] = e.a;
+            }
+            if (touched_n) touched_n[i] = c.tcount;
+        }
+        free(cand.v);
+        free(nn.v);
         scratch_free(&s);
     }
     return g->err ? -2 : 0;

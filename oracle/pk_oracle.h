@@ -55,6 +55,35 @@ int ora_search(const ora_graph *g, const void *queries, int64_t nq, int k, int e
 /* pickle::Distance for one pair (L2 squared or negative inner product). */
 float ora_distance(int dtype, int metric, const void *a, const void *b, int64_t dim);
 
+/* Summation order of float32 / float16 distances (integer types are exact in
+ * any order).  ORA_ORDER_SOURCE: the reference's source order (16 lanes, then
+ * a left-to-right lane sum; the default).  ORA_ORDER_DEVICE: the order of the
+ * device library's kernels, so that a search or build of the restatement can
+ * be replayed with the device's own distances.  Process-wide; set it before a
+ * call, not during one. */
+enum { ORA_ORDER_SOURCE = 0, ORA_ORDER_DEVICE = 1, ORA_ORDER_TABLE = 2 };
+void ora_set_float_order(int order);
+
+/* Fork detector for float parity.  Replays AnnSearch for each query with two
+ * sets of distances at once: order_a (ORA_ORDER_SOURCE or ORA_ORDER_DEVICE)
+ * drives every decision, and each comparison of two distances (SlideLayer's
+ * '<', the early exit, the admission test and every heap comparison) is also
+ * evaluated with order_b's distances (ORA_ORDER_SOURCE, ORA_ORDER_DEVICE, or
+ * ORA_ORDER_TABLE = values looked up per query in a table of (row key,
+ * distance) pairs, key = the row's external id or -1 for the zero row, keys
+ * sorted within each query's range tb_off[q]..tb_off[q+1]).  The first
+ * comparison whose outcome differs is the point where the two searches fork;
+ * fork[q*6 + 0..5] = {1 if forked else 0, where (1 slide, 2 early exit,
+ * 3 admission, 4 heap order; 5 a table lookup missed), the two operands in
+ * order a, the same two in order b}.  ids / dists (nq*k) are order_a's
+ * results (those of ora_search in that order).  touched (nullable,
+ * nq*touched_cap) receives the keys of the rows whose distances the order_a
+ * search evaluated, touched_n[q] their count (may exceed touched_cap: then
+ * the list is truncated). */
+int ora_search_fork(const ora_graph *g, const void *queries, int64_t nq, int k, int ef, int order_a, int order_b,
+                    const int64_t *tb_off, const int32_t *tb_key, const float *tb_val, int nthreads, int32_t *ids,
+                    float *dists, double *fork, int32_t *touched, int64_t touched_cap, int64_t *touched_n);
+
 /* The reference's level distribution: get_cumulative_probability(M)
  * (include/util.hpp:13-25).  Writes up to maxn values, returns the count. */
 int ora_cumulative_probability(int64_t M, double *out, int maxn);

@@ -18,12 +18,17 @@
 //       --threads 1 the build is then deterministic.
 //   search --graph g.pkg --queries Q.npy --k k --ef ef --threads t
 //          [--repeat r] [--dynamic] [--ids out.npy] [--dists out.npy] [--metrics]
+//          [--kq k.npy(int32) --efq ef.npy(int32)]
 //       Runs the batch AnnSearch (include/hnsw.hpp:528-541) timed with a
 //       steady clock around the whole batch, as benchmark/hnsw_pickle.cpp:79-86
 //       does, and the collect_metric pass (benchmark/hnsw_pickle.cpp:88-92).
 //       By default the distance kernels are instantiated with a fixed Dim
 //       for 96/100/128/200 like benchmark/hnsw_pickle.cpp:9-27 (the timed
 //       path); --dynamic uses std::dynamic_extent (the metric path).
+//       With --kq/--efq every query has its own k and ef: the batch loop of
+//       include/hnsw.hpp:528-541 (OpenMP dynamic,20) over the single-query
+//       AnnSearch (:509-525) with that query's values; --k is then the row
+//       width of --ids/--dists.
 //   dist   --a A.npy --b B.npy --metric l2|ip --out D.npy
 //       Row-wise pickle::Distance (include/distance.hpp:10-20) for KATs.
 #include <omp.h>
@@ -358,14 +363,36 @@ static int cmd_search(std::map<std::string, std::string> &a) {
     bool dynamic = a.count("dynamic") > 0;
     omp_set_num_threads(threads);
 
+    std::vector<int32_t> kq, efq;
+    if (a.count("kq") || a.count("efq")) {
+        pk_npy KQ, EQ;
+        if (pk_npy_read(a["kq"].c_str(), &KQ) != 0 || pk_npy_read(a["efq"].c_str(), &EQ) != 0 || KQ.word != 4 ||
+            EQ.word != 4 || (size_t)KQ.shape[0] != nq || (size_t)EQ.shape[0] != nq) {
+            fprintf(stderr, "bad --kq/--efq\n");
+            return 2;
+        }
+        kq.assign((int32_t *)KQ.data, (int32_t *)KQ.data + nq);
+        efq.assign((int32_t *)EQ.data, (int32_t *)EQ.data + nq);
+        free(KQ.data);
+        free(EQ.data);
+    }
+
     std::vector<std::vector<Entry>> results;
     std::vector<double> secs;
     type_switch(dtype, [&](auto *tp) {
         using T = std::remove_pointer_t<decltype(tp)>;
         dim_switch(dim, dynamic, [&](auto D) {
+            constexpr size_t Dim = decltype(D)::value;
             for (int r = 0; r < repeat; r++) {
                 auto t0 = std::chrono::steady_clock::now();
-                results = g->AnnSearch<T, decltype(D)::value, false>(k, ef, queries);
+                if (kq.empty()) {
+                    results = g->AnnSearch<T, Dim, false>(k, ef, queries);
+                } else {
+                    results.assign(nq, {});
+#pragma omp parallel for schedule(dynamic, 20)
+                    for (size_t i = 0; i < nq; i++)
+                        results[i] = g->AnnSearch<T, Dim, false>(kq[i], efq[i], queries.get_span<T, Dim>(i));
+                }
                 secs.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
             }
         });

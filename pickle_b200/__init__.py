@@ -74,6 +74,8 @@ def lib() -> ctypes.CDLL:
         L.pk_index_fast_timing.argtypes = [P, VP, VP]
         L.pk_index_tune_fast.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
         L.pk_index_search_noalloc.argtypes = [P, VP, I64, I32, I32, VP, VP, VP]
+        L.pk_index_search_var.argtypes = [P, VP, I64, VP, VP, I32, VP, VP]
+        L.pk_index_search_fast_host_var.argtypes = [P, VP, I64, VP, VP, I32, VP, VP, I32]
         L.pk_server_create.argtypes = [PP, P, ctypes.c_int, ctypes.c_int, I32, I32, I32, I32]
         L.pk_server_submit.argtypes = [P, VP, I32, I32, I32, ctypes.POINTER(ctypes.c_int64)]
         L.pk_server_wait.argtypes = [P, ctypes.c_int64, VP, VP, ctypes.POINTER(ctypes.c_double), I32]
@@ -85,6 +87,7 @@ def lib() -> ctypes.CDLL:
                      "pk_index_build", "pk_index_add", "pk_index_search", "pk_index_search_device",
                      "pk_index_save", "pk_index_load", "pk_index_info", "pk_index_layer", "pk_index_prepare_fast",
                      "pk_index_search_fast", "pk_index_search_fast_host", "pk_index_search_noalloc",
+                     "pk_index_search_var", "pk_index_search_fast_host_var",
                      "pk_server_create", "pk_server_submit", "pk_server_wait", "pk_server_stats",
                      "pk_server_set_watchdog", "pk_server_destroy", "pk_server_replay"]:
             getattr(L, name).restype = ctypes.c_int

@@ -173,6 +173,8 @@ struct pk_index {
     int32_t *d_fids = nullptr;
     float *d_fdists = nullptr;
     int64_t fids_n = 0, fdists_n = 0;
+    int32_t *d_karr = nullptr, *d_efarr = nullptr;  // per-query k / ef of host calls
+    int64_t karr_n = 0, efarr_n = 0;
     // walk launch shape (0 = the default): rows per fetch batch, log2 of the
     // visited-filter slots, warps per block
     int fast_rb = 0, fast_hlog2 = 0, fast_wpb = 0;
@@ -1034,6 +1036,8 @@ void destroy_handle(pk_index *h) {
     free_fast_ctx(h, h->fctx);
     cudaFree(h->d_fids);
     cudaFree(h->d_fdists);
+    cudaFree(h->d_karr);
+    cudaFree(h->d_efarr);
     cudaFree(h->d_qstage);
     cudaFree(h->d_ids);
     cudaFree(h->d_dists);
@@ -1135,6 +1139,46 @@ static int pk_index_search_impl(pk_index *h, const void *queries, int64_t nq, in
     PK_TRY(run_search(h, h->d_qstage, nq, k, ef, nullptr, nullptr, k, h->d_ids, h->d_dists, nullptr, s));
     PK_CUDA(cudaMemcpyAsync(out_ids, h->d_ids, sizeof(int32_t) * nq * k, cudaMemcpyDeviceToHost, s));
     PK_CUDA(cudaMemcpyAsync(out_dists, h->d_dists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    return PK_OK;
+}
+
+// Host buffers with a k and an ef per query (row i of the output holds
+// k_per_query[i] results, then -1 / FLT_MAX up to out_stride).
+static int pk_index_search_var_impl(pk_index *h, const void *queries, int64_t nq, const int32_t *k_per_query,
+                                    const int32_t *ef_per_query, int32_t out_stride, int32_t *out_ids,
+                                    float *out_dists) {
+    if (!h || nq < 0 || ((!queries || !out_ids || !out_dists || !k_per_query || !ef_per_query) && nq > 0))
+        return fail(PK_ERR_ARG, "bad arguments");
+    if (nq == 0) return PK_OK;
+    int32_t kmax = 0, efmax = 0;
+    for (int64_t i = 0; i < nq; i++) {
+        if (k_per_query[i] < 1 || ef_per_query[i] < 1) return fail(PK_ERR_ARG, "every k and ef must be >= 1");
+        kmax = std::max(kmax, k_per_query[i]);
+        efmax = std::max(efmax, ef_per_query[i]);
+    }
+    if (out_stride < kmax) return fail(PK_ERR_ARG, "out_stride below the largest k");
+    if (h->n0() == 0) {
+        for (int64_t i = 0; i < nq * out_stride; i++) {
+            out_ids[i] = -1;
+            out_dists[i] = FLT_MAX;
+        }
+        return PK_OK;
+    }
+    cudaStream_t s = h->stream;
+    PK_TRY(stage_queries(h, queries, nq, cudaMemcpyHostToDevice, s));
+    PK_TRY(ensure_buf(h, &h->d_ids, h->ids_n, nq * out_stride));
+    PK_TRY(ensure_buf(h, &h->d_dists, h->dists_n, nq * out_stride));
+    PK_TRY(ensure_buf(h, &h->d_karr, h->karr_n, nq));
+    PK_TRY(ensure_buf(h, &h->d_efarr, h->efarr_n, nq));
+    PK_CUDA(cudaMemcpyAsync(h->d_karr, k_per_query, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s));
+    PK_CUDA(cudaMemcpyAsync(h->d_efarr, ef_per_query, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s));
+    PK_CUDA(fill_i32(h->d_ids, nq * out_stride, -1, s));
+    PK_CUDA(fill_f32(h->d_dists, nq * out_stride, FLT_MAX, s));
+    PK_TRY(run_search(h, h->d_qstage, nq, kmax, efmax, h->d_karr, h->d_efarr, out_stride, h->d_ids, h->d_dists,
+                      nullptr, s));
+    PK_CUDA(cudaMemcpyAsync(out_ids, h->d_ids, sizeof(int32_t) * nq * out_stride, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaMemcpyAsync(out_dists, h->d_dists, sizeof(float) * nq * out_stride, cudaMemcpyDeviceToHost, s));
     PK_CUDA(cudaStreamSynchronize(s));
     return PK_OK;
 }
@@ -1489,6 +1533,44 @@ static int pk_index_search_fast_host_impl(pk_index *h, const void *queries, int6
                            nullptr, expand, s));
     PK_CUDA(cudaMemcpyAsync(out_ids, h->d_fids, sizeof(int32_t) * nq * k, cudaMemcpyDeviceToHost, s));
     PK_CUDA(cudaMemcpyAsync(out_dists, h->d_fdists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    return fast_status(h, h->fctx, s);
+}
+
+static int pk_index_search_fast_host_var_impl(pk_index *h, const void *queries, int64_t nq,
+                                              const int32_t *k_per_query, const int32_t *ef_per_query,
+                                              int32_t out_stride, int32_t *out_ids, float *out_dists,
+                                              int32_t expand) {
+    if (!h || nq < 0 || ((!queries || !out_ids || !out_dists || !k_per_query || !ef_per_query) && nq > 0))
+        return fail(PK_ERR_ARG, "bad arguments");
+    if (nq == 0) return PK_OK;
+    int32_t kmax = 0, efmax = 0;
+    for (int64_t i = 0; i < nq; i++) {
+        if (k_per_query[i] < 1 || ef_per_query[i] < 1) return fail(PK_ERR_ARG, "every k and ef must be >= 1");
+        kmax = std::max(kmax, k_per_query[i]);
+        efmax = std::max(efmax, ef_per_query[i]);
+    }
+    if (out_stride < kmax) return fail(PK_ERR_ARG, "out_stride below the largest k");
+    if (h->n0() == 0) {
+        for (int64_t i = 0; i < nq * out_stride; i++) {
+            out_ids[i] = -1;
+            out_dists[i] = FLT_MAX;
+        }
+        return PK_OK;
+    }
+    cudaStream_t s = h->stream;
+    PK_TRY(ensure_buf(h, &h->d_fids, h->fids_n, nq * out_stride));
+    PK_TRY(ensure_buf(h, &h->d_fdists, h->fdists_n, nq * out_stride));
+    PK_TRY(ensure_buf(h, &h->d_karr, h->karr_n, nq));
+    PK_TRY(ensure_buf(h, &h->d_efarr, h->efarr_n, nq));
+    PK_CUDA(cudaMemcpyAsync(h->d_karr, k_per_query, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s));
+    PK_CUDA(cudaMemcpyAsync(h->d_efarr, ef_per_query, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s));
+    PK_CUDA(fill_i32(h->d_fids, nq * out_stride, -1, s));
+    PK_CUDA(fill_f32(h->d_fdists, nq * out_stride, FLT_MAX, s));
+    PK_TRY(run_search_fast(h, h->fctx, queries, true, nq, kmax, efmax, h->d_karr, h->d_efarr, out_stride, h->d_fids,
+                           h->d_fdists, nullptr, expand, s));
+    PK_CUDA(cudaMemcpyAsync(out_ids, h->d_fids, sizeof(int32_t) * nq * out_stride, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaMemcpyAsync(out_dists, h->d_fdists, sizeof(float) * nq * out_stride, cudaMemcpyDeviceToHost, s));
     PK_CUDA(cudaStreamSynchronize(s));
     return fast_status(h, h->fctx, s);
 }
@@ -2076,6 +2158,30 @@ int pk_index_search_fast_host(pk_index *h, const void *queries, int64_t nq, int3
         return fail(PK_ERR_OOM, "host allocation failed");
     } catch (...) {
         return fail(PK_ERR_STATE, "pk_index_search_fast_host: unexpected exception");
+    }
+}
+
+int pk_index_search_var(pk_index *h, const void *queries, int64_t nq, const int32_t *k_per_query,
+                        const int32_t *ef_per_query, int32_t out_stride, int32_t *out_ids, float *out_dists) {
+    try {
+        return pk_index_search_var_impl(h, queries, nq, k_per_query, ef_per_query, out_stride, out_ids, out_dists);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_search_var: unexpected exception");
+    }
+}
+
+int pk_index_search_fast_host_var(pk_index *h, const void *queries, int64_t nq, const int32_t *k_per_query,
+                                  const int32_t *ef_per_query, int32_t out_stride, int32_t *out_ids,
+                                  float *out_dists, int32_t expand) {
+    try {
+        return pk_index_search_fast_host_var_impl(h, queries, nq, k_per_query, ef_per_query, out_stride, out_ids,
+                                                  out_dists, expand);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_search_fast_host_var: unexpected exception");
     }
 }
 

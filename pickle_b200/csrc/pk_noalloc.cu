@@ -20,7 +20,8 @@
 //    PK_ERR_OVERFLOW and the caller can fall back to pk_index_search_device.
 //  * The first call on a device looks up the array's device address there
 //    (with that device current); make that first call before any stream
-//    capture begins.
+//    capture begins.  Every call waits for its own work on the stream before
+//    it returns (it reads the overflow count back).
 //  * Every call on a device shares the one array, which keeps the previous
 //    call's contents.  What must start from zero is cleared by the call: the
 //    work counters on every call, and the visited bitmaps, which sit at the
@@ -116,8 +117,13 @@ int search_noalloc(const pk_index *h, const void *queries, int64_t nq, int32_t k
         wpb /= 2;
         smem = (size_t)wpb * pk::search_smem_per_warp(wcap, v.row_bytes);
     }
+    if (smem > 220 * 1024)
+        return fail(PK_ERR_ARG, "pk_index_search_noalloc: ef and the row size need more shared memory than a block has");
     const int nb = pk::search_blocks_per_sm(v.dtype, v.lc, wpb, smem);
-    if (nb <= 0) return fail(PK_ERR_CUDA, "pk_index_search_noalloc: search kernel cannot be resident");
+    if (nb <= 0) {
+        cudaGetLastError();
+        return fail(PK_ERR_CUDA, "pk_index_search_noalloc: search kernel cannot be resident");
+    }
     const int64_t bm_words = (v.lcap0 + 31) / 32 + 1;
     const int64_t vl_cap = std::max<int64_t>(4096, 16LL * ef);
     const int64_t tail = std::max<int64_t>(4096, 32LL * ef);
@@ -190,12 +196,23 @@ int search_noalloc(const pk_index *h, const void *queries, int64_t nq, int32_t k
                                  reinterpret_cast<int32_t *>(base + vl_off), (int32_t)vl_cap, base + tail_off,
                                  (int32_t)tail};
     a.wcap = wcap;
+    // a search that did not complete may leave marks in its bitmaps: the next
+    // call then clears the whole area again
+    auto forget_clean = [&]() {
+        std::lock_guard<std::mutex> lock(g_mu);
+        g_clean_bytes[v.device] = 0;
+    };
     cudaError_t e = pk::launch_search_exact(v.dg, v.dtype, v.lc, a, (int)(warps / wpb), wpb, smem, s);
-    if (e != cudaSuccess) return fail(PK_ERR_CUDA, "pk_index_search_noalloc: launch failed");
+    if (e != cudaSuccess) {
+        forget_clean();
+        return fail(PK_ERR_CUDA, "pk_index_search_noalloc: launch failed");
+    }
     int32_t over = 0;
     if (cudaMemcpyAsync(&over, base + 4, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        forget_clean();
         return fail(PK_ERR_CUDA, "pk_index_search_noalloc: kernel failed");
+    }
     if (over != 0)
         return fail(PK_ERR_OVERFLOW,
                     "pk_index_search_noalloc: some queries outgrew the fixed scratch; use pk_index_search_device");

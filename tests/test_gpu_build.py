@@ -17,15 +17,19 @@ from tests.helpers import case_data, levels_for
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", ["f32int_l2", "u8_ip", "i8_l2_d100"])
+@pytest.mark.parametrize("name", ["f32int_l2", "u8_ip", "i8_l2_d100", "f32unit_ip", "f16_l2"])
 def test_one_node_batches_equal_oracle_build(name, gpu):
+    """Float data too: the restatement builds with the device's float
+    summation order (the only difference between the two), and then every
+    array and every search answer is identical."""
     metric, base, queries, M, efc = case_data(name)
     n = 1500
     base = base[:n]
     order = np.random.default_rng(5).permutation(n).astype(np.int32)
     lv = levels_for(n, M, 5)
     g = oracle.OraGraph.new(metric, base.dtype, base.shape[1], M, efc, lv, oracle.GROWTH_CAPPED)
-    g.build(base, order)
+    with oracle.float_order(oracle.ORDER_DEVICE):
+        g.build(base, order)
     idx = HNSWIndex(base.shape[1], base.dtype, metric, M, efc)
     idx.set_levels(lv)
     idx.build(base, order, max_batch=1)
@@ -43,7 +47,8 @@ def test_one_node_batches_equal_oracle_build(name, gpu):
         np.testing.assert_array_equal(a["adj"][:n_l * cap], b["adj"][:n_l * cap])
         np.testing.assert_array_equal(a["dist"][:n_l * cap], b["dist"][:n_l * cap])
     # and the two graphs answer queries identically
-    oi, od = g.search(queries, 10, 40)
+    with oracle.float_order(oracle.ORDER_DEVICE):
+        oi, od = g.search(queries, 10, 40)
     ids, ds = idx.search(queries, 10, 40)
     np.testing.assert_array_equal(ids, oi)
     np.testing.assert_array_equal(ds, od)

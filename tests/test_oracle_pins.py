@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import CASES, INTEGER_CASES, case_data, compare_float_results, ref_graph
+from tests.helpers import (CASES, INTEGER_CASES, case_data, compare_float_results, mismatched_queries, ref_graph,
+                           reference_distance_table)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 GOLDEN_CASES = ["f32int_l2", "u8_ip", "i8_l2_d100", "f16_ip"]
@@ -78,7 +79,95 @@ def test_search_restatement_matches_reference(name, ref_bin):
         assert cnt[:, 4].sum() == info["base_dist"]
         assert cnt[:, 2].sum() + cnt[:, 5].sum() == info["neighbor"]
     else:
-        assert compare_float_results(oi, od, ri, rd) >= 0.98
+        # float sums are rounded differently by the reference's compiler:
+        # wherever the two sets of distances never disagree on a comparison
+        # the results must be the reference's; see the fork test below
+        assert len(mismatched_queries(oi, od, ri, rd)) <= 0.05 * len(queries)
+
+
+@pytest.mark.parametrize("name", sorted(set(CASES) - INTEGER_CASES))
+def test_float_search_forks_only_at_near_ties(name, ref_bin):
+    """The restatement replayed with the reference binary's own distances
+    (pk_ref dist, the instantiation its search runs) compared at every
+    decision: a query whose decisions never flip returns the reference's ids,
+    and every query whose ids differ from the reference's beyond 1e-6 ties
+    flips first at a comparison of two distances within 1e-6 of each other."""
+    metric, base, queries, M, efc = case_data(name)
+    path = ref_graph(name)
+    ri, rd, _ = oracle.ref_search(path, queries, 10, 32, threads=4)
+    g = oracle.OraGraph.load(path)
+    oi, od = g.search(queries, 10, 32, threads=4)
+    _, _, _, touched = g.search_fork(queries, 10, 32, oracle.ORDER_SOURCE, oracle.ORDER_SOURCE, threads=4,
+                                     touched_cap=100_000)
+    table = reference_distance_table(base, queries, touched, metric)
+    fi, fd, fork, _ = g.search_fork(queries, 10, 32, oracle.ORDER_SOURCE, oracle.ORDER_TABLE, table=table, threads=4)
+    np.testing.assert_array_equal(fi, oi)
+    np.testing.assert_array_equal(fd, od)
+    assert (fork[:, 1] != 5).all()
+    calm = fork[:, 0] == 0
+    np.testing.assert_array_equal(oi[calm], ri[calm])
+    for qi in mismatched_queries(oi, od, ri, rd):
+        f = fork[qi]
+        assert f[0] == 1.0
+        gap_a = abs(f[2] - f[3]) / max(abs(f[2]), abs(f[3]))
+        gap_b = abs(f[4] - f[5]) / max(abs(f[4]), abs(f[5]))
+        assert min(gap_a, gap_b) <= 1e-6, (qi, f)
+
+
+def test_fork_detector_consistency():
+    """Same order on both sides: no fork and the plain search's results; a
+    table holding the driving order's own distances: no fork either."""
+    metric, base, queries, M, efc = case_data("f32unit_ip")
+    path = ref_graph("f32unit_ip")
+    g = oracle.OraGraph.load(path)
+    for order in (oracle.ORDER_SOURCE, oracle.ORDER_DEVICE):
+        with oracle.float_order(order):
+            oi, od = g.search(queries, 10, 40, threads=4)
+        fi, fd, fork, touched = g.search_fork(queries, 10, 40, order, order, threads=4, touched_cap=100_000)
+        np.testing.assert_array_equal(fi, oi)
+        np.testing.assert_array_equal(fd, od)
+        assert (fork[:, 0] == 0).all()
+        keys = [np.unique(t) for t in touched]
+        off = np.zeros(len(keys) + 1, np.int64)
+        off[1:] = np.cumsum([len(x) for x in keys])
+        K = np.concatenate(keys).astype(np.int32)
+        qi = np.repeat(np.arange(len(keys)), [len(x) for x in keys])
+        with oracle.float_order(order):
+            vals = np.array([oracle.distance(metric, queries[i], base[k] if k >= 0 else np.zeros_like(base[0]))
+                             for i, k in zip(qi, K)], np.float32)
+        _, _, fork, _ = g.search_fork(queries, 10, 40, order, oracle.ORDER_TABLE, table=(off, K, vals), threads=4)
+        assert (fork[:, 0] == 0).all()
+    # the two orders do disagree somewhere, and where the results differ the
+    # search forked
+    with oracle.float_order(oracle.ORDER_DEVICE):
+        di, dd = g.search(queries, 10, 40, threads=4)
+    si, sd = g.search(queries, 10, 40, threads=4)
+    _, _, fork, _ = g.search_fork(queries, 10, 40, oracle.ORDER_DEVICE, oracle.ORDER_SOURCE, threads=4)
+    for q in np.nonzero((di != si).any(1))[0]:
+        assert fork[q, 0] == 1.0
+
+
+def test_device_order_distances():
+    """The device order's distances are float32 roundings of the exact value:
+    integer-valued rows give the exact integer, others agree with float64 to
+    a few units in the last place."""
+    rng = np.random.default_rng(4)
+    for dim in (32, 48, 96, 100, 128, 768):
+        ai = rng.integers(0, 256, size=(50, dim)).astype(np.float32)
+        bi = rng.integers(0, 256, size=(50, dim)).astype(np.float32)
+        af = rng.normal(size=(50, dim)).astype(np.float32)
+        bf = rng.normal(size=(50, dim)).astype(np.float32)
+        with oracle.float_order(oracle.ORDER_DEVICE):
+            for i in range(50):
+                assert oracle.distance("l2", ai[i], bi[i]) == float(((ai[i].astype(np.int64) - bi[i]) ** 2).sum())
+                for metric, exact in (("l2", ((af[i].astype(np.float64) - bf[i]) ** 2).sum()),
+                                      ("ip", -(af[i].astype(np.float64) * bf[i]).sum())):
+                    scale = (np.abs(af[i].astype(np.float64)) * np.abs(bf[i]) + (af[i].astype(np.float64) - bf[i]) ** 2).sum()
+                    assert abs(oracle.distance(metric, af[i], bf[i]) - exact) <= 1e-6 * scale
+                for dt in (np.float16,):
+                    x, y = af[i].astype(dt), bf[i].astype(dt)
+                    ex = ((x.astype(np.float64) - y) ** 2).sum()
+                    assert abs(oracle.distance("l2", x, y) - ex) <= 1e-6 * ex
 
 
 @pytest.mark.parametrize("name", ["f32int_l2", "u8_ip", "i8_l2_d100", "i8_ip"])

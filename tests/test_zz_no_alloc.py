@@ -14,7 +14,8 @@ import ctypes
 import numpy as np
 import pytest
 
-from pickle_b200 import HNSWIndex, lib
+import oracle
+from pickle_b200 import HNSWIndex, datasets, lib
 from tests.helpers import case_data, ref_graph
 
 pytestmark = pytest.mark.gpu
@@ -58,6 +59,53 @@ def test_noalloc_search_equals_device_search_on_two_calls(name, gpu, ref_bin):
         # any path that keeps the reference's heap order
         np.testing.assert_array_equal(ids.cpu().numpy(), want_ids.cpu().numpy())
         np.testing.assert_array_equal(ds.cpu().numpy(), want_ds.cpu().numpy())
+
+
+def _want(idx, q, k, ef):
+    import torch
+    ids = torch.empty((q.shape[0], k), dtype=torch.int32, device="cuda")
+    ds = torch.empty((q.shape[0], k), dtype=torch.float32, device="cuda")
+    idx.search_device(q, k, ef, ids, ds)
+    torch.cuda.synchronize()
+    return ids.cpu().numpy(), ds.cpu().numpy()
+
+
+def _got(idx, q, k, ef):
+    import torch
+    ids = torch.full((q.shape[0], k), -7, dtype=torch.int32, device="cuda")
+    ds = torch.zeros((q.shape[0], k), dtype=torch.float32, device="cuda")
+    rc = _call(idx, q, k, ef, ids, ds)
+    assert rc == 0, lib().pk_last_error()
+    torch.cuda.synchronize()
+    return ids.cpu().numpy(), ds.cpu().numpy()
+
+
+def test_noalloc_sequence_of_shapes_and_indexes(gpu, ref_bin):
+    """The fixed array keeps each call's leftovers: a few queries (few warps,
+    a small bitmap area), the whole batch (more warps: the bitmap area grows
+    over memory the previous call used for lists and spills), an index with a
+    larger layer 0 (larger bitmaps), then the first call again.  Every answer
+    equals pk_index_search_device's, and on integer data the oracle's."""
+    import torch
+    metric, base, queries, M, efc = case_data("u8_l2")
+    path = ref_graph("u8_l2")
+    a = HNSWIndex.load(path)
+    qa = torch.from_numpy(queries).cuda()
+    big_base, big_q = datasets.gmm_bytes(12000, 300, 64, ncomp=16, seed=5)
+    b = HNSWIndex(64, np.uint8, "l2", M=8, ef_construction=64)
+    b.set_seed(5)
+    b.build(big_base)
+    qb = torch.from_numpy(big_q).cuda()
+    oi, od = oracle.OraGraph.load(path).search(queries, 10, 40)
+    for idx, q, k, ef in [(a, qa[:4], 10, 40), (a, qa, 10, 40), (b, qb, 16, 200), (b, qb[:7], 5, 64),
+                          (a, qa[:4], 10, 40), (a, qa, 10, 40)]:
+        gi, gd = _got(idx, q, k, ef)
+        wi, wd = _want(idx, q, k, ef)
+        np.testing.assert_array_equal(gi, wi)
+        np.testing.assert_array_equal(gd, wd)
+        if idx is a:
+            np.testing.assert_array_equal(gi, oi[:q.shape[0]])
+            np.testing.assert_array_equal(gd, od[:q.shape[0]])
 
 
 def test_noalloc_refuses_requests_beyond_its_limits(gpu, ref_bin):
