@@ -89,6 +89,8 @@ def parse():
     p.add_argument("--paths", default="exact,f16", help="search paths to measure (exact, f16, fp8)")
     p.add_argument("--expand", type=int, default=1, help="entries expanded per step on the fast paths")
     p.add_argument("--fast-shape", default="", help="rows,filter_log2,warps for the fast walk instead of tuning")
+    p.add_argument("--launch-check", action="store_true",
+                   help="only start the ranks (gloo on the host), agree on the world size and exit")
     p.add_argument("--cache", default=os.environ.get("PK_BENCH_CACHE", os.path.join(tempfile.gettempdir(),
                                                                                    "pickle_b200_bench")),
                    help="directory for the built graph file, shared by both arms ('' = no cache)")
@@ -682,11 +684,35 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def launch_check(args):
+    """The process plumbing alone: every rank joins a gloo group, the world
+    size is checked against --gpus and agreed by an all-reduce."""
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE is {world}")
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+        t = torch.tensor([1.0])
+        dist.all_reduce(t)
+        seen = int(t.item())
+        dist.destroy_process_group()
+    else:
+        seen = 1
+    if rank == 0:
+        print(json.dumps({"launch_check": True, "world": world, "ranks_joined": seen}), flush=True)
+
+
 def main():
     args = parse()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(relaunch_distributed(args))
-    if args.impl == "reference":
+    if args.launch_check:
+        launch_check(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -71,7 +71,7 @@ int pk_index_create(pk_index **out, int metric, int dtype, int64_t dim, int64_t 
 int pk_index_destroy(pk_index *h);
 
 /* Sets the seed of the per-node level draw (default 0).  The reference draws
- * levels from std::random_device (include/util.hpp:172-198); here level(ext_id)
+ * levels from std::random_device (include/util.hpp:38-64); here level(ext_id)
  * is a pure function of (seed, ext_id) with the same distribution, so builds
  * are reproducible.  Must be called before the first insertion. */
 int pk_index_set_seed(pk_index *h, uint64_t seed);

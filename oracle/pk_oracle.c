@@ -8,7 +8,7 @@
  *
  * Floating-point summation order.  The reference computes float distances in
  * 16 SIMD lanes, lane l summing elements i = l (mod 16), and then adds the 16
- * lanes left to right (include/distance/avx512.hpp:187-251, Sum16 in
+ * lanes left to right (include/distance/avx512.hpp:187-231, Sum16 in
  * include/marco.hpp:128-131).  It is compiled with
  * -funsafe-math-optimizations, so the compiler may reassociate both steps, and
  * in practice its fixed-Dim and dynamic-extent instantiations of the same
@@ -354,7 +354,7 @@ static inline float dist_q(const ora_graph *g, const void *q, const void *row) {
 }
 
 /* ------------------------------------------------------------------ */
-/* visited sets: ByteMap, include/visited.hpp:540-589 (exact)           */
+/* visited sets: ByteMap, include/visited.hpp:248-297 (exact)           */
 /* ------------------------------------------------------------------ */
 
 typedef struct {

@@ -6,7 +6,7 @@
 // Tests and bench.py's CPU baseline run that binary as a subprocess; nothing
 // in the product links or calls it.  One graph per process, because the
 // reference's per-thread visited tables are sized on first use
-// (include/visited.hpp:558-562) and a second, taller graph in the same process
+// (include/visited.hpp:266-269) and a second, taller graph in the same process
 // would index past them.
 //
 // Commands (every array is a .npy file; see oracle/pk_npy.h):
@@ -14,7 +14,7 @@
 //          [--order ids.npy(int32)] [--levels lv.npy(uint8)] --out g.pkg
 //       Runs HNSWGraph::Build (include/hnsw.hpp:497-507).  --levels replaces the
 //       random_device level draw of InitBuffer (include/hnsw.hpp:222-245,
-//       include/util.hpp:172-198) so that a build can be reproduced; with
+//       include/util.hpp:38-64) so that a build can be reproduced; with
 //       --threads 1 the build is then deterministic.
 //   search --graph g.pkg --queries Q.npy --k k --ef ef --threads t
 //          [--repeat r] [--dynamic] [--ids out.npy] [--dists out.npy] [--metrics]

@@ -108,29 +108,98 @@ def _dev_ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
+class _class_or_instance:
+    """A method that works on the class (returning a new object) and on an
+    instance (acting on it), as HNSWIndex.load does."""
+
+    def __init__(self, fn):
+        self.fn = fn
+
+    def __get__(self, obj, owner):
+        def bound(*a, **kw):
+            return self.fn(owner, obj, *a, **kw)
+        bound.__doc__ = self.fn.__doc__
+        return bound
+
+
 class HNSWIndex:
     """An HNSW index resident in GPU memory.
 
-    HNSWIndex(dim, dtype, metric="l2", M=32, ef_construction=100) mirrors
-    HNSWGraph(max_degree, build_ef, DistFunc) (include/hnsw.hpp:27-36).
+    Two ways to make one:
+      HNSWIndex(dim, dtype, metric="l2", M=32, ef_construction=100) mirrors
+        HNSWGraph(max_degree, build_ef, DistFunc) (include/hnsw.hpp:27-36): the
+        index exists at once, empty.
+      HNSWIndex() mirrors the reference's Python binding (pybind/hnsw.cpp:
+        116-127): set the properties search_ef (100), build_ef (100), top_k
+        (10), M (32) and metric, then build(data) creates the index with the
+        data's dimension and type (a later build(data) replaces it, as there).
+    search(queries) uses top_k and search_ef and returns the ids, nq x top_k;
+    search(queries, k, ef) returns (ids, distances).
     """
 
     def __init__(self, dim: int = 0, dtype=np.float32, metric: str = "l2", M: int = 32,
                  ef_construction: int = 100, _handle=None):
         self._h = None
+        self._deferred = False
+        self.search_ef = 100
+        self.top_k = 10
+        self.metric = metric
+        self._M = M
+        self._build_ef = ef_construction
         if _handle is not None:
-            self._h = _handle
-        else:
+            self._adopt(_handle)
+        elif dim > 0:
             h = ctypes.c_void_p()
             _check(lib().pk_index_create(ctypes.byref(h), METRICS[metric], DTYPES[np.dtype(dtype)], dim, M,
                                          ef_construction))
-            self._h = h
+            self._adopt(h)
+        else:
+            # the reference binding's default constructor: created by build()
+            self._deferred = True
+            self.dim = 0
+            self.dtype = None
+
+    def _adopt(self, h) -> None:
+        self.close()
+        self._h = h
         info = self.info()
         self.dim = info["dim"]
         self.dtype = NP_OF[info["dtype"]]
         self.metric = {1: "l2", 2: "ip"}[info["metric"]]
-        self.M = info["M"]
-        self.ef_construction = info["ef_construction"]
+        self._M = info["M"]
+        self._build_ef = info["ef_construction"]
+
+    # ---- the reference binding's properties (pybind/hnsw.cpp:118-123) ----
+    @property
+    def M(self) -> int:
+        return self._M
+
+    @M.setter
+    def M(self, value: int) -> None:
+        if self._h is not None and not self._deferred:
+            raise ValueError("M is fixed once the index exists (it was given to the constructor)")
+        self._M = int(value)
+
+    @property
+    def build_ef(self) -> int:
+        return self._build_ef
+
+    @build_ef.setter
+    def build_ef(self, value: int) -> None:
+        if self._h is not None and not self._deferred:
+            raise ValueError("build_ef is fixed once the index exists (it was given to the constructor)")
+        self._build_ef = int(value)
+
+    @property
+    def ef_construction(self) -> int:
+        return self._build_ef
+
+    @property
+    def num_layer(self) -> int:
+        """Layers of the graph (0 before a build).  The reference binding binds
+        this name to its top_k getter by mistake (pybind/hnsw.cpp:123); here it
+        is the layer count its getNumLayer computes (:46)."""
+        return self.info()["num_layers"] if self._h is not None else 0
 
     def __del__(self):
         self.close()
@@ -149,7 +218,21 @@ class HNSWIndex:
         _check(lib().pk_index_set_levels(self._h, _ptr(lv), len(lv)))
 
     def build(self, data: np.ndarray, ext_ids: np.ndarray | None = None, max_batch: int = 0) -> None:
-        """HNSWGraph::Build: insert data[ext_ids[i]] with id ext_ids[i], i = 0..n-1."""
+        """HNSWGraph::Build: insert data[ext_ids[i]] with id ext_ids[i], i = 0..n-1
+        (ext_ids None: 0..n-1).  On a default-constructed index this first
+        creates the index from the data's shape and type and the M, build_ef
+        and metric properties, replacing any earlier one."""
+        if self._deferred:
+            data = np.ascontiguousarray(data)
+            if data.ndim != 2 or data.dtype not in DTYPES:
+                raise ValueError("build expects a 2-D uint8, int8, float16 or float32 array")
+            h = ctypes.c_void_p()
+            _check(lib().pk_index_create(ctypes.byref(h), METRICS[self.metric], DTYPES[data.dtype], data.shape[1],
+                                         self._M, self._build_ef))
+            self.close()
+            self._h = h
+            self.dim = data.shape[1]
+            self.dtype = data.dtype
         data = self._rows(data)
         ids = None if ext_ids is None else np.ascontiguousarray(ext_ids, dtype=np.int32)
         _check(lib().pk_index_build(self._h, _ptr(data), data.shape[0], _ptr(ids) if ids is not None else None,
@@ -164,13 +247,35 @@ class HNSWIndex:
         _check(lib().pk_index_add(self._h, _ptr(rows), rows.shape[0], _ptr(ids), max_batch))
 
     # ---- queries --------------------------------------------------------
-    def search(self, queries: np.ndarray, k: int, ef: int):
-        """HNSWGraph::AnnSearch(k, ef, queries): (ids, dists), each nq x k, ascending."""
+    def search(self, queries: np.ndarray, k: int | None = None, ef: int | None = None):
+        """HNSWGraph::AnnSearch(k, ef, queries).  With k and ef: (ids, dists),
+        each nq x k, ascending.  Without them: the reference binding's
+        search(query) (pybind/hnsw.cpp:73-101), k = top_k and ef = search_ef,
+        returning the ids only."""
         q = self._rows(queries)
         nq = q.shape[0]
-        ids = np.empty((nq, k), np.int32)
-        dists = np.empty((nq, k), np.float32)
-        _check(lib().pk_index_search(self._h, _ptr(q), nq, k, ef, _ptr(ids), _ptr(dists)))
+        kk = self.top_k if k is None else k
+        ee = self.search_ef if ef is None else ef
+        ids = np.empty((nq, kk), np.int32)
+        dists = np.empty((nq, kk), np.float32)
+        _check(lib().pk_index_search(self._h, _ptr(q), nq, kk, ee, _ptr(ids), _ptr(dists)))
+        if k is None and ef is None:
+            return ids
+        return ids, dists
+
+    def search_var(self, queries: np.ndarray, k_per_query: np.ndarray, ef_per_query: np.ndarray):
+        """AnnSearch with a k and an ef per query (host buffers): (ids, dists),
+        nq x max(k); row i holds k_per_query[i] results, then -1 / FLT_MAX."""
+        q = self._rows(queries)
+        kq = np.ascontiguousarray(k_per_query, np.int32)
+        eq = np.ascontiguousarray(ef_per_query, np.int32)
+        if len(kq) != q.shape[0] or len(eq) != q.shape[0]:
+            raise ValueError("one k and one ef per query")
+        stride = int(kq.max()) if len(kq) else 1
+        ids = np.empty((q.shape[0], stride), np.int32)
+        dists = np.empty((q.shape[0], stride), np.float32)
+        _check(lib().pk_index_search_var(self._h, _ptr(q), q.shape[0], _ptr(kq), _ptr(eq), stride, _ptr(ids),
+                                         _ptr(dists)))
         return ids, dists
 
     def search_device(self, queries, k: int, ef: int, out_ids, out_dists, k_per_query=None, ef_per_query=None,
@@ -229,6 +334,21 @@ class HNSWIndex:
                                           _dev_ptr(ef_per_query), out_ids.shape[1], _dev_ptr(out_ids),
                                           _dev_ptr(out_dists), _dev_ptr(counters), expand, s))
 
+    def search_fast_var(self, queries: np.ndarray, k_per_query: np.ndarray, ef_per_query: np.ndarray,
+                        expand: int = 1):
+        """search_fast with a k and an ef per query: (ids, dists), nq x max(k)."""
+        q = self._rows(queries)
+        kq = np.ascontiguousarray(k_per_query, np.int32)
+        eq = np.ascontiguousarray(ef_per_query, np.int32)
+        if len(kq) != q.shape[0] or len(eq) != q.shape[0]:
+            raise ValueError("one k and one ef per query")
+        stride = int(kq.max()) if len(kq) else 1
+        ids = np.empty((q.shape[0], stride), np.int32)
+        dists = np.empty((q.shape[0], stride), np.float32)
+        _check(lib().pk_index_search_fast_host_var(self._h, _ptr(q), q.shape[0], _ptr(kq), _ptr(eq), stride,
+                                                   _ptr(ids), _ptr(dists), expand))
+        return ids, dists
+
     def search_fast(self, queries: np.ndarray, k: int, ef: int, expand: int = 1):
         """Low-precision walk + exact re-rank with host buffers: (ids, dists)."""
         q = self._rows(queries)
@@ -242,11 +362,18 @@ class HNSWIndex:
     def save(self, path: str) -> None:
         _check(lib().pk_index_save(self._h, os.fsencode(path)))
 
-    @classmethod
-    def load(cls, path: str) -> "HNSWIndex":
+    @_class_or_instance
+    def load(cls, self, path: str) -> "HNSWIndex":
+        """HNSWIndex.load(path) returns a new index read from a graph file;
+        index.load(path) replaces this index's graph with the file's, as the
+        reference binding's load does (pybind/hnsw.cpp:108-110)."""
         h = ctypes.c_void_p()
         _check(lib().pk_index_load(ctypes.byref(h), os.fsencode(path)))
-        return cls(_handle=h)
+        if self is None:
+            return cls(_handle=h)
+        self._deferred = False
+        self._adopt(h)
+        return self
 
     # ---- introspection --------------------------------------------------
     def info(self) -> dict:
@@ -274,6 +401,8 @@ class HNSWIndex:
                 "has_vector": hv, "adj": adj, "dist": dist}
 
     def _rows(self, a: np.ndarray) -> np.ndarray:
+        if self._h is None:
+            raise RuntimeError("the index has not been built or loaded")
         a = np.ascontiguousarray(a)
         if a.ndim != 2 or a.shape[1] != self.dim:
             raise ValueError(f"expected (n, {self.dim}) rows, got {a.shape}")

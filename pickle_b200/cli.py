@@ -93,6 +93,8 @@ def cmd_search(a):
             _log(a.log_path, f"k={k} search_ef={ef} recall={recall:.1f} qps/t={int(nq / secs)} "
                              f"hop={c[0] + c[3]:.1f} dist={c[1] + c[4]:.1f} base_hop={c[3]:.1f} "
                              f"base_dist={c[4]:.1f} build_ef={idx.ef_construction} thread=1")
+            if a.out_ids:
+                np.save(a.out_ids, ids.cpu().numpy())
 
 
 def cmd_gen(a):
@@ -152,6 +154,7 @@ def main(argv=None):
     s.add_argument("--path", default="exact", choices=["exact", "f16", "fp8"],
                    help="exact: the reference's search; f16/fp8: low-precision walk + exact re-rank")
     s.add_argument("--expand", type=int, default=1)
+    s.add_argument("--out_ids", default="", help="save the ids of the last (k, ef) searched as .npy")
     g = sub.add_parser("gen")
     g.add_argument("--config", required=True)
     g.add_argument("--out", required=True)

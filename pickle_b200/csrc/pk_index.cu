@@ -352,7 +352,7 @@ std::vector<double> cumulative_probability(int64_t M) {
 
 // The level of one node: a fresh uniform draw per level, compared with the
 // cumulative probability (the scheme of get_random_levels,
-// include/util.hpp:172-198), from a stream keyed by (seed, external id).
+// include/util.hpp:38-64), from a stream keyed by (seed, external id).
 int draw_level(const std::vector<double> &cp, uint64_t seed, int32_t ext) {
     uint64_t s = seed ^ (0xD1B54A32D192ED03ULL * (uint64_t)(uint32_t)ext + 0x8CB92BA72F3D8DD7ULL);
     for (size_t l = 0; l < cp.size(); l++) {

@@ -4,7 +4,7 @@
 // Reference behaviour reproduced here (juelinl/pickle):
 //   Distance         include/distance.hpp:10-20, include/distance/avx512.hpp
 //   EntryHeap        include/queue.hpp:99-289  (push / pop / tie order)
-//   ByteMap          include/visited.hpp:540-589 (exact visited set)
+//   ByteMap          include/visited.hpp:248-297 (exact visited set)
 //   SlideLayer       include/hnsw.hpp:446-494
 //   SearchLayer(Fast) include/hnsw.hpp:304-444
 //

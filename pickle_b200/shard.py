@@ -36,30 +36,46 @@ def query_slice(nq: int, rank: int, world: int) -> Tuple[int, int]:
     return lo, lo + base + (1 if rank < extra else 0)
 
 
-def merge_topk(ids: np.ndarray, dists: np.ndarray, k: int) -> Tuple[np.ndarray, np.ndarray]:
-    """Merge S candidate lists per query ([S, nq, kk] each, -1 = empty) into
-    the k best by (distance, id), ascending; -1 / +inf pad short rows."""
+def merge_topk_tensors(ids, dists, k: int):
+    """Merge S candidate lists per query (torch tensors [S, nq, kk], -1 =
+    empty) into the k best by (distance, id), ascending, each id once; -1 /
+    +inf pad short rows.  Runs where the tensors are (the GPU after an NCCL
+    all-gather): two stable sorts give the (distance, id) order, and an id
+    listed by two shards (the same row, so the same distance) lands twice in
+    a row and keeps its first copy."""
+    import torch
     s, nq, kk = ids.shape
-    ii = np.transpose(ids, (1, 0, 2)).reshape(nq, s * kk).astype(np.int64)
-    dd = np.transpose(dists, (1, 0, 2)).reshape(nq, s * kk).astype(np.float64)
-    dd = np.where(ii < 0, np.inf, dd)
-    ii_key = np.where(ii < 0, np.iinfo(np.int64).max, ii)
-    out_i = np.full((nq, k), -1, np.int32)
-    out_d = np.full((nq, k), np.inf, np.float32)
-    for r in range(nq):
-        order = np.lexsort((ii_key[r], dd[r]))
-        seen = set()
-        j = 0
-        for c in order:
-            if ii[r, c] < 0 or j == k:
-                break
-            if ii[r, c] in seen:
-                continue
-            seen.add(int(ii[r, c]))
-            out_i[r, j] = ii[r, c]
-            out_d[r, j] = dd[r, c]
-            j += 1
+    ii = ids.permute(1, 0, 2).reshape(nq, s * kk).to(torch.int64)
+    dd = dists.permute(1, 0, 2).reshape(nq, s * kk).to(torch.float64)
+    empty = ii < 0
+    dd = torch.where(empty, torch.full_like(dd, float("inf")), dd)
+    idkey = torch.where(empty, torch.full_like(ii, torch.iinfo(torch.int64).max), ii)
+    o1 = torch.argsort(idkey, dim=1, stable=True)
+    o2 = torch.argsort(torch.gather(dd, 1, o1), dim=1, stable=True)
+    order = torch.gather(o1, 1, o2)
+    si = torch.gather(ii, 1, order)
+    sd = torch.gather(dd, 1, order)
+    drop = si < 0
+    drop[:, 1:] |= si[:, 1:] == si[:, :-1]
+    keep = torch.argsort(drop.to(torch.int8), dim=1, stable=True)[:, :k]
+    out_i = torch.gather(si, 1, keep)
+    out_d = torch.gather(sd, 1, keep)
+    bad = torch.gather(drop, 1, keep)
+    out_i = torch.where(bad, torch.full_like(out_i, -1), out_i).to(torch.int32)
+    out_d = torch.where(bad, torch.full_like(out_d, float("inf")), out_d).to(torch.float32)
+    if out_i.shape[1] < k:
+        pad = k - out_i.shape[1]
+        out_i = torch.cat([out_i, torch.full((nq, pad), -1, dtype=torch.int32, device=out_i.device)], 1)
+        out_d = torch.cat([out_d, torch.full((nq, pad), float("inf"), device=out_d.device)], 1)
     return out_i, out_d
+
+
+def merge_topk(ids: np.ndarray, dists: np.ndarray, k: int) -> Tuple[np.ndarray, np.ndarray]:
+    """merge_topk_tensors on numpy arrays ([S, nq, kk] each)."""
+    import torch
+    oi, od = merge_topk_tensors(torch.from_numpy(np.ascontiguousarray(ids)),
+                                torch.from_numpy(np.ascontiguousarray(dists)), k)
+    return oi.numpy(), od.numpy()
 
 
 def _comm_device(group):
@@ -104,16 +120,40 @@ def replica_search(search: SearchFn, queries: np.ndarray, k: int, group=None, ga
     return np.concatenate(_all_gather_rows(ids, group)), np.concatenate(_all_gather_rows(ds, group))
 
 
-def sharded_search(search: SearchFn, queries: np.ndarray, k: int, id_offset: int, group=None):
-    """Base-sharded: search the whole batch on this rank's shard (ids local to
-    the shard, shifted by id_offset to global ids), all-gather every shard's
-    top-k, merge by (distance, id).  Every rank returns the merged result."""
+def sharded_search_tensors(search, queries, k: int, id_offset: int, group=None):
+    """Base-sharded on torch tensors: search(queries) returns this shard's
+    (ids int32, dists float32) tensors, [nq, >= k], ids local to the shard;
+    they are shifted by id_offset to global ids, every shard's top-k is
+    all-gathered (one NCCL all_gather per array on GPU tensors, over
+    NVLink/NVSwitch; gloo on CPU tensors) and merged where the tensors are.
+    Every rank returns the merged (ids, dists)."""
+    import torch
+    import torch.distributed as dist
     ids, ds = search(queries)
-    ids = np.where(ids[:, :k] >= 0, ids[:, :k].astype(np.int64) + id_offset, -1).astype(np.int32)
-    ds = np.ascontiguousarray(ds[:, :k], np.float32)
-    all_i = np.stack(_all_gather_rows(np.ascontiguousarray(ids), group))
-    all_d = np.stack(_all_gather_rows(ds, group))
-    return merge_topk(all_i, all_d, k)
+    ids = ids[:, :k].to(torch.int64)
+    ids = torch.where(ids >= 0, ids + id_offset, torch.full_like(ids, -1)).to(torch.int32).contiguous()
+    ds = ds[:, :k].to(torch.float32).contiguous()
+    world = dist.get_world_size(group)
+    all_i = [torch.empty_like(ids) for _ in range(world)]
+    all_d = [torch.empty_like(ds) for _ in range(world)]
+    dist.all_gather(all_i, ids, group=group)
+    dist.all_gather(all_d, ds, group=group)
+    return merge_topk_tensors(torch.stack(all_i), torch.stack(all_d), k)
+
+
+def sharded_search(search: SearchFn, queries: np.ndarray, k: int, id_offset: int, group=None):
+    """Base-sharded with numpy in and out: search the whole batch on this
+    rank's shard, all-gather and merge as sharded_search_tensors does (on the
+    rank's GPU for NCCL groups).  Every rank returns the merged result."""
+    import torch
+    dev = _comm_device(group)
+
+    def run(q):
+        i, d = search(q.cpu().numpy())
+        return torch.from_numpy(np.ascontiguousarray(i)).to(dev), torch.from_numpy(np.ascontiguousarray(d)).to(dev)
+
+    oi, od = sharded_search_tensors(run, torch.from_numpy(np.ascontiguousarray(queries)), k, id_offset, group)
+    return oi.cpu().numpy(), od.cpu().numpy()
 
 
 def max_over_ranks(value: float, group=None) -> float:

@@ -1,14 +1,17 @@
 // Uses the header-only C++ front end the way a caller of pickle::v2::HNSWGraph
 // would: Build from an NDArray, AnnSearch a batch, Serializer round trip.
-// Prints "ids <first row>" or "error <code>".
+// Prints "ids <first row>" or "error <code>".  argv[1]: where to write the
+// graph file (default: pk_cpp_demo.pkg in the working directory).
 #include <cstdio>
 #include <random>
+#include <string>
 
 #include "pickle_b200/hnsw.hpp"
 
 using namespace pickle_b200;
 
-int main() {
+int main(int argc, char **argv) {
+    const std::string path = argc > 1 ? argv[1] : "pk_cpp_demo.pkg";
     const size_t n = 2000, dim = 32, nq = 16;
     std::mt19937 rng(1);
     std::uniform_int_distribution<int> u(0, 255);
@@ -26,8 +29,8 @@ int main() {
         g.SetSeed(1);
         g.Build<float>(ext, all);
         auto res = g.AnnSearch<float>(5, 32, queries);
-        Serializer::to_disk("/tmp/pk_cpp_demo.pkg", g);
-        HNSWGraph h = Serializer::from_disk("/tmp/pk_cpp_demo.pkg");
+        Serializer::to_disk(path, g);
+        HNSWGraph h = Serializer::from_disk(path);
         auto res2 = h.AnnSearch<float>(5, 32, queries);
         bool same = res.size() == res2.size();
         for (size_t i = 0; same && i < res.size(); i++)

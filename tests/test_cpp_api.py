@@ -23,7 +23,7 @@ def _build(tmp_path):
 def test_cpp_front_end_compiles_and_reports_status(tmp_path):
     import torch
     exe = _build(tmp_path)
-    p = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    p = subprocess.run([exe, str(tmp_path / "g.pkg")], capture_output=True, text=True, timeout=300)
     if torch.cuda.is_available():
         assert p.returncode == 0, p.stdout + p.stderr
     else:
@@ -33,7 +33,7 @@ def test_cpp_front_end_compiles_and_reports_status(tmp_path):
 @pytest.mark.gpu
 def test_cpp_front_end_on_gpu(tmp_path, gpu):
     exe = _build(tmp_path)
-    p = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    p = subprocess.run([exe, str(tmp_path / "g.pkg")], capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stdout + p.stderr
     first = p.stdout.split("\n")[0].split()
     assert first[0] == "ids" and first[1] == "0"  # the query is row 0 itself

@@ -83,3 +83,25 @@ def test_merge_topk_orders_by_distance_then_id_and_pads():
     mi, md = shard.merge_topk(ids, ds, 5)
     np.testing.assert_array_equal(mi, [[9, 2, 5, 1, -1]])          # 1 listed twice is kept once
     np.testing.assert_array_equal(md, [[0.5, 1.0, 1.0, 3.0, np.inf]])
+
+
+def test_bench_relaunches_itself_for_n_gpus():
+    """bench.py --gpus 2 without a torch.distributed environment reruns itself
+    under torch.distributed.run with two processes (here on gloo, host only);
+    both ranks join and agree on the world size."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                             "MASTER_PORT")}
+    p = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--launch-check"],
+                       capture_output=True, text=True, timeout=300, env=env)
+    assert p.returncode == 0, p.stdout + p.stderr
+    line = json.loads([x for x in p.stdout.splitlines() if x.startswith("{")][-1])
+    assert line == {"launch_check": True, "world": 2, "ranks_joined": 2}
+    # a world size that disagrees with --gpus is refused
+    env2 = dict(env, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    q = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--launch-check"],
+                       capture_output=True, text=True, timeout=300, env=env2)
+    assert q.returncode != 0 and "WORLD_SIZE" in q.stderr
