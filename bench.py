@@ -388,6 +388,8 @@ def run_ours(args):
         return total, float(np.mean(kernel_ms)), clk.summary()
 
     def tune(path, k, ef, mixed):
+        """The walk's launch shape: one for a uniform batch, one per list-width
+        class for the mixed batch (returned as {class: shape})."""
         if path == "exact":
             return None
         if args.fast_shape:
@@ -395,8 +397,19 @@ def run_ours(args):
             idx.set_fast_params(*shape)
             return shape
         nt = min(nq, 20_000)
+        if mixed:
+            per = idx.tune_fast_classes(q_dev[:nt // 2], k, ef, args.expand, stream)
+            return {c: v[0] for c, v in per.items()}
         shape, _ = idx.tune_fast(q_dev[:nt], k, ef, args.expand, stream)
         return shape
+
+    def apply_shape(shape):
+        if isinstance(shape, dict):
+            idx.set_fast_params(0, 0, 0)
+            for c, sh in shape.items():
+                idx.set_fast_class_params(c, *sh)
+        elif shape is not None:
+            idx.set_fast_params(*shape)
 
     def counts(path, k, ef, mixed, shape):
         """Per-query means of the six work counters; for the fast paths with a
@@ -409,11 +422,11 @@ def run_ours(args):
         fetched = cnt.double().mean(0).cpu().numpy()
         if path == "exact":
             return fetched, fetched
-        idx.set_fast_params(shape[0], 15, 1)
+        idx.set_fast_params(16, 15, 1)
         cnt.zero_()
         call(path, k, ef, mixed, counters=cnt)
         torch.cuda.synchronize()
-        idx.set_fast_params(*shape)
+        apply_shape(shape)
         return cnt.double().mean(0).cpu().numpy(), fetched
 
     elem = {"f16": 2, "f32": 4}[w["dtype"]]
@@ -450,7 +463,7 @@ def run_ours(args):
                     "kernel_ms": kms10, "clocks": clk10}
         if w["mixed"]:
             efmax = int(efq.max())
-            shape = tune(path, 100, 384, False)
+            shape = tune(path, kmax, efmax, True)
             tot, kms, clk = timed(path, kmax, efmax, True)
             call(path, kmax, efmax, True)
             torch.cuda.synchronize()
@@ -484,7 +497,7 @@ def run_ours(args):
     dh = torch.empty((nq, stride), dtype=torch.float32).pin_memory()
     ef_u = best["k10"]["ef"]
     if bp != "exact":
-        idx.set_fast_params(*(bh["launch_shape"]))
+        apply_shape(bh["launch_shape"])
 
     def host_call():
         qp, ip_, dp = (ctypes.c_void_p(t.data_ptr()) for t in (qh, ih, dh))

@@ -167,7 +167,8 @@ int pk_index_search_fast_host_var(pk_index *h, const void *queries, int64_t nq, 
  * min(32, 12 KiB / row)); filter_log2 = log2 of the slots of the per-query
  * table of recently seen ids (5..15; default 10); warps_per_block (1..8;
  * default 4).  The results do not depend on the shape (the table only saves
- * recomputed distances); the speed does.  No counterpart in the reference. */
+ * recomputed distances); the speed does.  Clears the per-class shapes of
+ * pk_index_tune_fast_classes.  No counterpart in the reference. */
 int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter_log2, int32_t warps_per_block);
 
 /* Measurement: with timing enabled, each pk_index_search_fast /
@@ -188,6 +189,24 @@ int pk_index_fast_timing(pk_index *h, float *walk_ms, float *rerank_ms);
  * the same as with any other shape.  No counterpart in the reference. */
 int pk_index_tune_fast(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t expand,
                        int32_t *out_shape, float *out_ms, void *stream);
+
+/* Autotuner for batches whose queries carry their own ef: the walk runs one
+ * launch per list width (1, 2, 3, 4, 6, 8, 12, 16 slots of 32 entries per
+ * lane), and this tunes each width class up to max_ef separately on the given
+ * queries (each class at its widest ef, k = min(k, that ef)), keeping one
+ * launch shape per class.  out_shapes (8 x 3 ints, may be null) receives
+ * rows_per_batch, filter_log2, warps_per_block per class (zeros for classes
+ * above max_ef), out_ms (8 floats, may be null) each class's batch time.
+ * pk_index_set_fast_params and pk_index_tune_fast clear the per-class shapes.
+ * No counterpart in the reference. */
+int pk_index_tune_fast_classes(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t max_ef,
+                               int32_t expand, int32_t *out_shapes, float *out_ms, void *stream);
+
+/* Sets the launch shape of one list-width class (0..7, see above) as
+ * pk_index_tune_fast_classes would; all three values 0 = the handle's shape.
+ * No counterpart in the reference. */
+int pk_index_set_fast_class_params(pk_index *h, int32_t width_class, int32_t rows_per_batch, int32_t filter_log2,
+                                   int32_t warps_per_block);
 
 /* Serving: continuous batching over pk_index_search_fast.  No counterpart
  * in the reference (its batch AnnSearch is a blocking OpenMP loop,

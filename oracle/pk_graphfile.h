@@ -50,7 +50,15 @@
  *                          node's vector equals its layer-0 row
  *                          (include/hnsw_layer.hpp:304-307), so upper layers
  *                          store only has_vector.
- *   uint64   checksum      FNV-1a 64 over every preceding byte
+ *   uint64   checksum      version 1: FNV-1a 64 over every preceding byte.
+ *                          version 2 (same layout; written by the device
+ *                          library): the preceding bytes in blocks of 4 MiB,
+ *                          each block's digest FNV-1a 64 over its
+ *                          little-endian 64-bit words (the last one zero
+ *                          padded) and then its length, the checksum FNV-1a 64
+ *                          over the block digests and then the total length -
+ *                          the blocks can be verified in parallel.
+ * Both versions are read here; pkf_write writes version 1.
  */
 #ifndef PK_ORACLE_GRAPHFILE_H
 #define PK_ORACLE_GRAPHFILE_H
@@ -91,18 +99,81 @@ static inline int pkf_elem_size(int dtype) {
     }
 }
 
+#define PKF_FNV_BASIS 1469598103934665603ULL
+#define PKF_FNV_PRIME 1099511628211ULL
+#define PKF_BLOCK ((uint64_t)4 << 20)
+
+/* The version 2 checksum, computed over a stream of bytes. */
+typedef struct {
+    uint64_t file_h, blk_h, total, word, blk_len;
+    unsigned wfill;
+} pkf_bh;
+
+static inline void pkf_bh_init(pkf_bh *b) {
+    b->file_h = b->blk_h = PKF_FNV_BASIS;
+    b->total = b->word = b->blk_len = 0;
+    b->wfill = 0;
+}
+static inline void pkf_bh_close_block(pkf_bh *b) {
+    if (b->wfill) {
+        b->blk_h = (b->blk_h ^ b->word) * PKF_FNV_PRIME;
+        b->word = 0;
+        b->wfill = 0;
+    }
+    b->blk_h = (b->blk_h ^ b->blk_len) * PKF_FNV_PRIME;
+    b->file_h = (b->file_h ^ b->blk_h) * PKF_FNV_PRIME;
+    b->blk_h = PKF_FNV_BASIS;
+    b->blk_len = 0;
+}
+static inline void pkf_bh_update(pkf_bh *b, const void *p, size_t n) {
+    const unsigned char *c = (const unsigned char *)p;
+    while (n) {
+        uint64_t room = PKF_BLOCK - b->blk_len;
+        size_t take = n < room ? n : (size_t)room, i = 0;
+        for (; i < take && b->wfill; i++) {
+            b->word |= (uint64_t)c[i] << (8 * b->wfill);
+            if (++b->wfill == 8) {
+                b->blk_h = (b->blk_h ^ b->word) * PKF_FNV_PRIME;
+                b->word = 0;
+                b->wfill = 0;
+            }
+        }
+        for (; i + 8 <= take; i += 8) {
+            uint64_t w;
+            memcpy(&w, c + i, 8);
+            b->blk_h = (b->blk_h ^ w) * PKF_FNV_PRIME;
+        }
+        for (; i < take; i++) b->word |= (uint64_t)c[i] << (8 * b->wfill++);
+        b->blk_len += take;
+        b->total += take;
+        c += take;
+        n -= take;
+        if (b->blk_len == PKF_BLOCK) pkf_bh_close_block(b);
+    }
+}
+static inline uint64_t pkf_bh_final(pkf_bh *b) {
+    if (b->blk_len) pkf_bh_close_block(b);
+    return (b->file_h ^ b->total) * PKF_FNV_PRIME;
+}
+
 typedef struct {
     FILE *f;
     uint64_t h;
     int err;
+    int version;
+    pkf_bh bh;
 } pkf_io;
 
 static inline void pkf_hash(pkf_io *io, const void *p, size_t n) {
+    if (io->version == 2) {
+        pkf_bh_update(&io->bh, p, n);
+        return;
+    }
     const unsigned char *b = (const unsigned char *)p;
     uint64_t h = io->h;
     for (size_t i = 0; i < n; i++) {
         h ^= b[i];
-        h *= 1099511628211ULL;
+        h *= PKF_FNV_PRIME;
     }
     io->h = h;
 }
@@ -137,7 +208,11 @@ static inline void pkf_free(pkf_graph *g) {
 }
 
 static inline int pkf_write(const char *path, const pkf_graph *g) {
-    pkf_io io = {fopen(path, "wb"), 1469598103934665603ULL, 0};
+    pkf_io io;
+    memset(&io, 0, sizeof(io));
+    io.f = fopen(path, "wb");
+    io.h = PKF_FNV_BASIS;
+    io.version = 1;
     if (!io.f) return -1;
     char magic[8] = PKF_MAGIC;
     uint32_t version = 1, flags = 0;
@@ -179,15 +254,20 @@ static inline int pkf_write(const char *path, const pkf_graph *g) {
  * -4 bad header values, -5 checksum mismatch, -6 out of memory. */
 static inline int pkf_read(const char *path, pkf_graph *g) {
     memset(g, 0, sizeof(*g));
-    pkf_io io = {fopen(path, "rb"), 1469598103934665603ULL, 0};
+    pkf_io io;
+    memset(&io, 0, sizeof(io));
+    io.f = fopen(path, "rb");
+    io.h = PKF_FNV_BASIS;
     if (!io.f) return -1;
-    char magic[8];
+    char head[16];
     uint32_t version, flags;
-    pkf_r(&io, magic, 8);
-    pkf_r(&io, &version, 4);
-    pkf_r(&io, &flags, 4);
-    if (io.err) { fclose(io.f); return -2; }
-    if (memcmp(magic, PKF_MAGIC, 8) != 0 || version != 1) { fclose(io.f); return -3; }
+    if (fread(head, 1, 16, io.f) != 16) { fclose(io.f); return -2; }
+    memcpy(&version, head + 8, 4);
+    memcpy(&flags, head + 12, 4);
+    if (memcmp(head, PKF_MAGIC, 8) != 0 || (version != 1 && version != 2)) { fclose(io.f); return -3; }
+    io.version = (int)version;
+    pkf_bh_init(&io.bh);
+    pkf_hash(&io, head, 16);
     pkf_r(&io, &g->metric, 4);
     pkf_r(&io, &g->dtype, 4);
     pkf_r(&io, &g->dim, 8);
@@ -241,7 +321,7 @@ static inline int pkf_read(const char *path, pkf_graph *g) {
     g->vectors = malloc(vb ? vb : 1);
     if (!g->vectors) { pkf_free(g); fclose(io.f); return -6; }
     pkf_r(&io, g->vectors, vb);
-    uint64_t want = io.h, got = 0;
+    uint64_t want = io.version == 2 ? pkf_bh_final(&io.bh) : io.h, got = 0;
     if (io.err || fread(&got, 1, 8, io.f) != 8) { pkf_free(g); fclose(io.f); return -2; }
     fclose(io.f);
     if (got != want) { pkf_free(g); return -5; }

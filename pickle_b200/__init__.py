@@ -73,6 +73,8 @@ def lib() -> ctypes.CDLL:
         L.pk_index_set_fast_timing.argtypes = [P, ctypes.c_int]
         L.pk_index_fast_timing.argtypes = [P, VP, VP]
         L.pk_index_tune_fast.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
+        L.pk_index_tune_fast_classes.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
+        L.pk_index_set_fast_class_params.argtypes = [P, I32, I32, I32, I32]
         L.pk_index_search_noalloc.argtypes = [P, VP, I64, I32, I32, VP, VP, VP]
         L.pk_index_search_var.argtypes = [P, VP, I64, VP, VP, I32, VP, VP]
         L.pk_index_search_fast_host_var.argtypes = [P, VP, I64, VP, VP, I32, VP, VP, I32]
@@ -87,7 +89,8 @@ def lib() -> ctypes.CDLL:
                      "pk_index_build", "pk_index_add", "pk_index_search", "pk_index_search_device",
                      "pk_index_save", "pk_index_load", "pk_index_info", "pk_index_layer", "pk_index_prepare_fast",
                      "pk_index_search_fast", "pk_index_search_fast_host", "pk_index_search_noalloc",
-                     "pk_index_search_var", "pk_index_search_fast_host_var",
+                     "pk_index_search_var", "pk_index_search_fast_host_var", "pk_index_tune_fast_classes",
+                     "pk_index_set_fast_class_params",
                      "pk_server_create", "pk_server_submit", "pk_server_wait", "pk_server_stats",
                      "pk_server_set_watchdog", "pk_server_destroy", "pk_server_replay"]:
             getattr(L, name).restype = ctypes.c_int
@@ -324,6 +327,24 @@ class HNSWIndex:
         _check(lib().pk_index_tune_fast(self._h, _dev_ptr(queries), queries.shape[0], k, ef, expand, _ptr(shape),
                                         _ptr(ms), s))
         return tuple(int(x) for x in shape), float(ms[0])
+
+    def tune_fast_classes(self, queries, k: int, max_ef: int, expand: int = 1, stream=None):
+        """Tune one walk launch shape per list-width class up to max_ef on these
+        queries (a torch CUDA tensor), for batches with per-query ef; returns
+        {class index: ((rows_per_batch, filter_log2, warps_per_block), ms)}."""
+        shapes = np.zeros(24, np.int32)
+        ms = np.zeros(8, np.float32)
+        s = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _check(lib().pk_index_tune_fast_classes(self._h, _dev_ptr(queries), queries.shape[0], k, max_ef, expand,
+                                                _ptr(shapes), _ptr(ms), s))
+        return {c: (tuple(int(x) for x in shapes[3 * c:3 * c + 3]), float(ms[c])) for c in range(8)
+                if shapes[3 * c] > 0}
+
+    def set_fast_class_params(self, width_class: int, rows_per_batch: int = 0, filter_log2: int = 0,
+                              warps_per_block: int = 0) -> None:
+        """Launch shape of one list-width class (all zeros: the handle's shape)."""
+        _check(lib().pk_index_set_fast_class_params(self._h, width_class, rows_per_batch, filter_log2,
+                                                    warps_per_block))
 
     def search_fast_device(self, queries, k: int, ef: int, out_ids, out_dists, k_per_query=None, ef_per_query=None,
                            counters=None, expand: int = 1, stream=None) -> None:

@@ -178,6 +178,9 @@ struct pk_index {
     // walk launch shape (0 = the default): rows per fetch batch, log2 of the
     // visited-filter slots, warps per block
     int fast_rb = 0, fast_hlog2 = 0, fast_wpb = 0;
+    // per list-width class (pk::slot_class): a shape that overrides the one
+    // above for that class's launch (0 = none)
+    int cls_rb[pk::kSlotClasses] = {}, cls_hlog2[pk::kSlotClasses] = {}, cls_wpb[pk::kSlotClasses] = {};
     bool fast_timing = false;      // record events around the walk and the re-rank
 
     size_t dev_bytes = 0;
@@ -823,11 +826,15 @@ struct WalkShape {
     int idbits;
     size_t smem;
 };
-int walk_shape(const pk_index *h, WalkShape &w) {
+int walk_shape(const pk_index *h, WalkShape &w, int cls = -1) {
     const int64_t trb = h->trav_row_bytes;
-    w.rb = h->fast_rb > 0 ? h->fast_rb : (int)std::max<int64_t>(8, std::min<int64_t>(32, 12288 / trb));
-    w.hlog2 = h->fast_hlog2 > 0 ? h->fast_hlog2 : 10;
-    w.wpb = h->fast_wpb > 0 ? h->fast_wpb : 4;
+    const bool own = cls >= 0 && cls < pk::kSlotClasses && h->cls_rb[cls] > 0;
+    const int rb = own ? h->cls_rb[cls] : h->fast_rb;
+    const int hl = own ? h->cls_hlog2[cls] : h->fast_hlog2;
+    const int wp = own ? h->cls_wpb[cls] : h->fast_wpb;
+    w.rb = rb > 0 ? rb : (int)std::max<int64_t>(8, std::min<int64_t>(32, 12288 / trb));
+    w.hlog2 = hl > 0 ? hl : 10;
+    w.wpb = wp > 0 ? wp : 4;
     const int64_t ids = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
     w.tag16 = pk::seen_tag16(ids, w.hlog2);
     w.idbits = std::max(pk::idbits_for(ids), w.hlog2 - 2);
@@ -855,7 +862,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     // its own launch, so a query pays for the list it needs
     const bool binned = ef_arr != nullptr && slots > 1;
     WalkShape ws;
-    PK_TRY(walk_shape(h, ws));
+    PK_TRY(walk_shape(h, ws, pk::slot_class(ef)));
     PK_TRY(ensure_buf(h, &c.d_work, c.work_n, kWorkInts));
     PK_TRY(ensure_buf(h, &c.d_cand, c.cand_n, nq * cs));
     if (binned) PK_TRY(ensure_buf(h, &c.d_lists, c.lists_n, nq * pk::kSlotClasses));
@@ -885,10 +892,6 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     a.status = c.d_work + kWorkStatus;
     a.cand = c.d_cand;
     a.cand_stride = cs;
-    a.rb = ws.rb;
-    a.hlog2 = ws.hlog2;
-    a.tag16 = ws.tag16 ? 1 : 0;
-    a.idbits = ws.idbits;
     a.tq_rows = c.d_tq;
     a.tq_row_bytes = tq_rb;
     a.qnorm = c.d_qn;
@@ -906,6 +909,11 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
         const int sl = pk::slot_class_width(cls);
         if (!binned && sl != slots) continue;
+        PK_TRY(walk_shape(h, ws, cls));
+        a.rb = ws.rb;
+        a.hlog2 = ws.hlog2;
+        a.tag16 = ws.tag16 ? 1 : 0;
+        a.idbits = ws.idbits;
         const int nb = pk::walk_blocks_per_sm(h->trav, sl, a.expand, ws.wpb, ws.smem);
         if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
         const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + ws.wpb - 1) / ws.wpb);
@@ -1255,23 +1263,39 @@ static int pk_index_save_impl(const pk_index *hc, const char *path) {
     return PK_OK;
 }
 
+// Maps the file, checks it, and uploads each array from the mapping to the
+// device (the large ones - adjacency, distances, vectors - with no host copy).
 static int pk_index_load_impl(pk_index **out, const char *path) {
     if (!out || !path) return fail(PK_ERR_ARG, "bad arguments");
     *out = nullptr;
-    pk::FileGraph g;
+    pk::MappedGraph g;
     std::string err;
-    int rc = pk::read_graph_file(path, g, err);
+    int rc = pk::map_graph_file(path, g, err);
     if (rc != PK_OK) return fail(rc, err);
-    // consistency checks the reference would trip over (ids, ranges)
     const int nl = (int)g.layers.size();
     if (nl > pk::kMaxLayers) return fail(PK_ERR_FORMAT, "too many layers");
+    // the small per-node arrays, read out of the (unaligned) mapping
+    std::vector<std::vector<int32_t>> ext(nl), deg(nl), heu(nl);
+    std::vector<std::vector<uint8_t>> hasv(nl);
     for (int l = 0; l < nl; l++) {
-        const pk::FileLayer &F = g.layers[l];
+        const pk::MappedLayer &F = g.layers[l];
+        ext[l].resize(F.n);
+        deg[l].resize(F.n);
+        heu[l].resize(F.n);
+        hasv[l].resize(F.n);
+        std::vector<int16_t> d16(F.n), h16(F.n);
+        std::memcpy(ext[l].data(), F.ext, 4 * (size_t)F.n);
+        std::memcpy(d16.data(), F.degree, 2 * (size_t)F.n);
+        std::memcpy(h16.data(), F.heuristic, 2 * (size_t)F.n);
+        std::memcpy(hasv[l].data(), F.has_vector, (size_t)F.n);
+        // consistency checks the reference would trip over (ids, ranges)
         if (F.cap != (l == 0 ? 2 * g.max_degree : g.max_degree)) return fail(PK_ERR_FORMAT, "unexpected layer cap");
         if (F.n > 0 && (F.ent < 0 || F.ent >= F.layer_capacity)) return fail(PK_ERR_FORMAT, "bad entry id");
         for (int64_t i = 0; i < F.n; i++) {
-            if (F.ext[i] < 0 || F.ext[i] >= g.capacity) return fail(PK_ERR_FORMAT, "external id out of range");
-            if (F.degree[i] < 0 || F.heuristic[i] < 0) return fail(PK_ERR_FORMAT, "negative degree");
+            if (ext[l][i] < 0 || ext[l][i] >= g.capacity) return fail(PK_ERR_FORMAT, "external id out of range");
+            if (d16[i] < 0 || h16[i] < 0) return fail(PK_ERR_FORMAT, "negative degree");
+            deg[l][i] = d16[i];
+            heu[l][i] = h16[i];
         }
     }
     pk_index *h = new (std::nothrow) pk_index();
@@ -1291,40 +1315,38 @@ static int pk_index_load_impl(pk_index **out, const char *path) {
     h->ext_level.assign(g.capacity, 0);
     std::vector<std::vector<int32_t>> ext2in(nl);
     for (int l = 0; l < nl; l++) {
-        const pk::FileLayer &F = g.layers[l];
+        const pk::MappedLayer &F = g.layers[l];
         ext2in[l].assign(g.capacity, -1);
         for (int64_t i = 0; i < F.n; i++) {
-            ext2in[l][F.ext[i]] = (int32_t)i;
-            h->ext_level[F.ext[i]] = (uint8_t)l;
+            ext2in[l][ext[l][i]] = (int32_t)i;
+            h->ext_level[ext[l][i]] = (uint8_t)l;
         }
     }
     if (nl > 0)
-        for (int64_t i = 0; i < g.layers[0].n; i++) h->ext_in0[g.layers[0].ext[i]] = (int32_t)i;
+        for (int64_t i = 0; i < g.layers[0].n; i++) h->ext_in0[ext[0][i]] = (int32_t)i;
     for (int l = 0; l < nl; l++) {
-        const pk::FileLayer &F = g.layers[l];
+        const pk::MappedLayer &F = g.layers[l];
         // spare rows after the last node so that a spilled list read past the
         // end meets -1 entries (skipped) rather than unallocated memory
         int64_t need = F.layer_capacity;
-        for (int64_t i = 0; i < F.n; i++) need = std::max(need, (i * F.cap + F.degree[i] + F.cap - 1) / F.cap);
+        for (int64_t i = 0; i < F.n; i++) need = std::max(need, (i * F.cap + deg[l][i] + F.cap - 1) / F.cap);
         if ((rc = ensure_layer(h, l, need, F.cap)) != PK_OK) return bail(rc);
         pk::DevLayer &L = h->hg.L[l];
         L.lcap = F.layer_capacity;
         L.n = F.n;
         L.ent = F.ent;
-        std::vector<int32_t> deg(F.n), heu(F.n), vrow(F.n, -1), down(F.n, -1);
-        for (int64_t i = 0; i < F.n; i++) {
-            deg[i] = F.degree[i];
-            heu[i] = F.heuristic[i];
-            if (l > 0) {
-                vrow[i] = F.has_vector[i] ? h->ext_in0[F.ext[i]] : -1;
-                down[i] = ext2in[l - 1][F.ext[i]];
+        std::vector<int32_t> vrow(F.n, -1), down(F.n, -1);
+        if (l > 0)
+            for (int64_t i = 0; i < F.n; i++) {
+                vrow[i] = hasv[l][i] ? h->ext_in0[ext[l][i]] : -1;
+                down[i] = ext2in[l - 1][ext[l][i]];
             }
-        }
-        if (cudaMemcpy(L.ext, F.ext.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(L.deg, deg.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(L.heu, heu.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(L.adj, F.adj.data(), 4 * F.adj.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(L.dist, F.dist.data(), 4 * F.dist.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        const size_t e = (size_t)(F.layer_capacity * F.cap);
+        if (cudaMemcpy(L.ext, ext[l].data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.deg, deg[l].data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.heu, heu[l].data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.adj, F.adj, 4 * e, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(L.dist, F.dist, 4 * e, cudaMemcpyHostToDevice) != cudaSuccess ||
             (l > 0 && cudaMemcpy(L.vrow, vrow.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess) ||
             (l > 0 && cudaMemcpy(L.down, down.data(), 4 * F.n, cudaMemcpyHostToDevice) != cudaSuccess))
             return bail(fail(PK_ERR_CUDA, "upload failed"));
@@ -1333,7 +1355,7 @@ static int pk_index_load_impl(pk_index **out, const char *path) {
     const int64_t lcap0 = nl > 0 ? g.layers[0].layer_capacity : 0;
     if ((rc = ensure_vec(h, std::max<int64_t>(lcap0, 1))) != PK_OK) return bail(rc);
     const size_t w = (size_t)(h->dim * h->esz);
-    if (n0 > 0 && cudaMemcpy2D((void *)h->hg.vec0, (size_t)h->row_bytes, g.vectors.data(), w, w, (size_t)n0,
+    if (n0 > 0 && cudaMemcpy2D((void *)h->hg.vec0, (size_t)h->row_bytes, g.vectors, w, w, (size_t)n0,
                                cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(PK_ERR_CUDA, "vector upload failed"));
     h->hg.enter_level = nl > 0 ? g.enter_level : 0;
@@ -1405,38 +1427,36 @@ static int pk_index_prepare_fast_impl(pk_index *h, int traversal) {
     return build_traversal(h, traversal == PK_TRAVERSAL_F16 ? pk::kTravF16 : pk::kTravE4M3);
 }
 
-// Times the walk + re-rank of this batch for a grid of launch shapes (rows
-// per fetch batch, visited-filter size, warps per block) and keeps the
-// fastest.  The result lists are the same for every shape; only the work
-// and its overlap change, so the choice is by time alone.
-static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
-                                   int32_t expand, int32_t *out_shape, float *out_ms, void *stream) {
-    if (!h || !queries || nq < 1 || k < 1 || ef < k) return fail(PK_ERR_ARG, "bad arguments");
-    if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
-    if (h->n0() == 0) return fail(PK_ERR_STATE, "the index is empty");
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
+// Times the walk + re-rank of this batch (uniform k and ef) for a grid of
+// launch shapes (rows per fetch batch, visited-filter size, warps per block)
+// and returns the fastest.  The result lists are the same for every shape;
+// only the work and its overlap change, so the choice is by time alone.  The
+// shapes are tried as the shape of ef's list-width class, which is left as it
+// was.  reps = timed runs per shape (after one warm-up run).
+int tune_shape(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t expand, int reps,
+               cudaStream_t s, int &brb, int &bh, int &bw, float &best) {
     PK_TRY(ensure_buf(h, &h->d_fids, h->fids_n, nq * k));
     PK_TRY(ensure_buf(h, &h->d_fdists, h->fdists_n, nq * k));
-    const int keep_rb = h->fast_rb, keep_h = h->fast_hlog2, keep_w = h->fast_wpb;
+    const int cls = pk::slot_class(ef);
+    const int keep_rb = h->cls_rb[cls], keep_h = h->cls_hlog2[cls], keep_w = h->cls_wpb[cls];
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     PK_CUDA(cudaEventCreate(&e0));
     if (cudaEventCreate(&e1) != cudaSuccess) {
         cudaEventDestroy(e0);
         return fail(PK_ERR_CUDA, "cudaEventCreate failed");
     }
-    float best = -1.f;
-    int brb = 0, bh = 0, bw = 0;
+    best = -1.f;
+    brb = bh = bw = 0;
     int rc = PK_OK;
-    // times one shape (the first of three runs warms caches); false if it
-    // does not fit or a launch failed (rc set)
+    // times one shape; false if it does not fit or a launch failed (rc set)
     auto time_shape = [&](int rb, int hl, int wp) -> bool {
-        h->fast_rb = rb;
-        h->fast_hlog2 = hl;
-        h->fast_wpb = wp;
+        h->cls_rb[cls] = rb;
+        h->cls_hlog2[cls] = hl;
+        h->cls_wpb[cls] = wp;
         WalkShape ws;
-        if (walk_shape(h, ws) != PK_OK || ws.wpb != wp) return false;
+        if (walk_shape(h, ws, cls) != PK_OK || ws.wpb != wp) return false;
         float ms = 0.f;
-        for (int rep = 0; rep < 3 && rc == PK_OK; rep++) {
+        for (int rep = 0; rep <= reps && rc == PK_OK; rep++) {
             if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(PK_ERR_CUDA, "cudaEventRecord failed");
             if (rc == PK_OK)
                 rc = run_search_fast(h, h->fctx, queries, false, nq, k, ef, nullptr, nullptr, k, h->d_fids,
@@ -1451,7 +1471,7 @@ static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq,
         // a walk that stopped early on a fetch timeout must not look fast
         if (rc == PK_OK) rc = fast_status(h, h->fctx, s);
         if (rc != PK_OK) return false;
-        ms /= 2.f;
+        ms /= (float)reps;
         if (best < 0.f || ms < best) {
             best = ms;
             brb = rb;
@@ -1478,22 +1498,70 @@ static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq,
         if (rc == PK_OK && best >= 0.f && rb != r1) time_shape(rb, h1, w1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    h->cls_rb[cls] = keep_rb;
+    h->cls_hlog2[cls] = keep_h;
+    h->cls_wpb[cls] = keep_w;
     if (rc == PK_OK) rc = fast_status(h, h->fctx, s);
-    if (rc != PK_OK || best < 0.f) {
-        h->fast_rb = keep_rb;
-        h->fast_hlog2 = keep_h;
-        h->fast_wpb = keep_w;
-        return rc != PK_OK ? rc : fail(PK_ERR_ARG, "no launch shape fits this index");
-    }
-    h->fast_rb = brb;
-    h->fast_hlog2 = bh;
-    h->fast_wpb = bw;
+    if (rc != PK_OK) return rc;
+    if (best < 0.f) return fail(PK_ERR_ARG, "no launch shape fits this index");
+    return PK_OK;
+}
+
+static int tune_check(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef) {
+    if (!h || !queries || nq < 1 || k < 1 || ef < k) return fail(PK_ERR_ARG, "bad arguments");
+    if (ef > pk::kFastMaxEf) return fail(PK_ERR_ARG, "ef too large for the fast path");
+    if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
+    if (h->n0() == 0) return fail(PK_ERR_STATE, "the index is empty");
+    return PK_OK;
+}
+
+// Tunes at this batch's ef and keeps the winner as the handle's shape for
+// every list width (the per-class shapes are cleared).
+static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
+                                   int32_t expand, int32_t *out_shape, float *out_ms, void *stream) {
+    PK_TRY(tune_check(h, queries, nq, k, ef));
+    int rb = 0, hl = 0, wp = 0;
+    float ms = 0.f;
+    PK_TRY(tune_shape(h, queries, nq, k, ef, expand, 2, static_cast<cudaStream_t>(stream), rb, hl, wp, ms));
+    h->fast_rb = rb;
+    h->fast_hlog2 = hl;
+    h->fast_wpb = wp;
+    for (int c = 0; c < pk::kSlotClasses; c++) h->cls_rb[c] = h->cls_hlog2[c] = h->cls_wpb[c] = 0;
     if (out_shape) {
-        out_shape[0] = brb;
-        out_shape[1] = bh;
-        out_shape[2] = bw;
+        out_shape[0] = rb;
+        out_shape[1] = hl;
+        out_shape[2] = wp;
     }
-    if (out_ms) *out_ms = best;
+    if (out_ms) *out_ms = ms;
+    return PK_OK;
+}
+
+// Tunes every list-width class up to max_ef on this batch (each at the widest
+// ef of its class, k = min(k, that ef)) and keeps one shape per class, for
+// batches whose queries carry their own ef.
+static int pk_index_tune_fast_classes_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t max_ef,
+                                           int32_t expand, int32_t *out_shapes, float *out_ms, void *stream) {
+    PK_TRY(tune_check(h, queries, nq, std::min(k, max_ef), max_ef));
+    for (int c = 0; c < pk::kSlotClasses; c++) {
+        if (out_shapes) out_shapes[3 * c] = out_shapes[3 * c + 1] = out_shapes[3 * c + 2] = 0;
+        if (out_ms) out_ms[c] = 0.f;
+        const int lo = c == 0 ? 1 : 32 * pk::slot_class_width(c - 1) + 1;
+        if (lo > max_ef) continue;
+        const int ef = std::min(32 * pk::slot_class_width(c), std::min(max_ef, pk::kFastMaxEf));
+        int rb = 0, hl = 0, wp = 0;
+        float ms = 0.f;
+        PK_TRY(tune_shape(h, queries, nq, std::min(k, ef), ef, expand, 1, static_cast<cudaStream_t>(stream), rb, hl,
+                          wp, ms));
+        h->cls_rb[c] = rb;
+        h->cls_hlog2[c] = hl;
+        h->cls_wpb[c] = wp;
+        if (out_shapes) {
+            out_shapes[3 * c] = rb;
+            out_shapes[3 * c + 1] = hl;
+            out_shapes[3 * c + 2] = wp;
+        }
+        if (out_ms) out_ms[c] = ms;
+    }
     return PK_OK;
 }
 
@@ -2131,7 +2199,35 @@ int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter
     h->fast_rb = rows_per_batch;
     h->fast_hlog2 = filter_log2;
     h->fast_wpb = warps_per_block;
+    for (int c = 0; c < pk::kSlotClasses; c++) h->cls_rb[c] = h->cls_hlog2[c] = h->cls_wpb[c] = 0;
     return PK_OK;
+}
+
+int pk_index_set_fast_class_params(pk_index *h, int32_t width_class, int32_t rows_per_batch, int32_t filter_log2,
+                                   int32_t warps_per_block) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    if (width_class < 0 || width_class >= pk::kSlotClasses) return fail(PK_ERR_ARG, "width_class must be 0..7");
+    if (rows_per_batch < 0 || rows_per_batch > 256) return fail(PK_ERR_ARG, "rows_per_batch must be 0..256");
+    if (filter_log2 != 0 && (filter_log2 < 5 || filter_log2 > 15))
+        return fail(PK_ERR_ARG, "filter_log2 must be 0 or 5..15");
+    if (warps_per_block < 0 || warps_per_block > 8) return fail(PK_ERR_ARG, "warps_per_block must be 0..8");
+    if ((rows_per_batch == 0) != (filter_log2 == 0) || (rows_per_batch == 0) != (warps_per_block == 0))
+        return fail(PK_ERR_ARG, "give all three values, or all three 0 to fall back to the handle's shape");
+    h->cls_rb[width_class] = rows_per_batch;
+    h->cls_hlog2[width_class] = filter_log2;
+    h->cls_wpb[width_class] = warps_per_block;
+    return PK_OK;
+}
+
+int pk_index_tune_fast_classes(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t max_ef,
+                               int32_t expand, int32_t *out_shapes, float *out_ms, void *stream) {
+    try {
+        return pk_index_tune_fast_classes_impl(h, queries, nq, k, max_ef, expand, out_shapes, out_ms, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(PK_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_index_tune_fast_classes: unexpected exception");
+    }
 }
 
 int pk_index_set_fast_timing(pk_index *h, int enable) {

@@ -66,6 +66,16 @@ def test_saved_build_reloads_identically(gpu, tmp_path):
     i2, d2 = again.search(queries, 10, 40)
     np.testing.assert_array_equal(ids, i2)
     np.testing.assert_array_equal(ds, d2)
+    # the device library writes version 2 (block checksum) and checks it on load
+    raw = open(p, "rb").read()
+    assert int.from_bytes(raw[8:12], "little") == 2
+    from tests.test_oracle_pins import v2_checksum
+    assert int.from_bytes(raw[-8:], "little") == v2_checksum(raw[:-8])
+    bad = bytearray(raw)
+    bad[len(bad) // 2] ^= 4
+    open(p + ".bad", "wb").write(bytes(bad))
+    with pytest.raises(Exception):
+        HNSWIndex.load(p + ".bad")
     # the oracle reads the device library's file and answers the same
     g = oracle.OraGraph.load(p)
     oi, od = g.search(queries, 10, 40)

@@ -255,3 +255,44 @@ def test_level_distribution_formula():
         want = np.cumsum([np.exp(-l / r) * (1 - np.exp(-1 / r)) for l in range(len(cp))])
         np.testing.assert_allclose(cp, want, rtol=1e-12)
         assert np.exp(-len(cp) / r) * (1 - np.exp(-1 / r)) < 1e-9
+
+
+def v2_checksum(payload: bytes) -> int:
+    """The version 2 graph-file checksum, restated from its definition: 4 MiB
+    blocks, each digested as FNV-1a 64 over little-endian 64-bit words (last
+    word zero padded) and then its length; FNV-1a 64 over the digests, then
+    the total length."""
+    P, B, M = 1099511628211, 4 << 20, (1 << 64) - 1
+    h = 1469598103934665603
+    for b0 in range(0, len(payload), B):
+        blk = payload[b0:b0 + B]
+        pad = blk + b"\0" * (-len(blk) % 8)
+        d = 1469598103934665603
+        for w in np.frombuffer(pad, "<u8").tolist():
+            d = ((d ^ w) * P) & M
+        d = ((d ^ len(blk)) * P) & M
+        h = ((h ^ d) * P) & M
+    return ((h ^ len(payload)) * P) & M
+
+
+def test_graph_file_version_2_block_checksum(tmp_path):
+    """A version 2 file (the device library's format: block checksum) is read
+    by the oracle like the version 1 file it was made from; a flipped byte
+    is caught."""
+    src = open(os.path.join(GOLDEN, "u8_ip.pkg"), "rb").read()
+    body = bytearray(src[:-8])
+    body[8:12] = (2).to_bytes(4, "little")
+    v2 = bytes(body) + v2_checksum(bytes(body)).to_bytes(8, "little")
+    p = str(tmp_path / "v2.pkg")
+    open(p, "wb").write(v2)
+    z = np.load(os.path.join(GOLDEN, "u8_ip.npz"))
+    meta = json.loads(str(z["meta"]))
+    a = oracle.OraGraph.load(os.path.join(GOLDEN, "u8_ip.pkg")).search(z["queries"], meta["k"], meta["ef"])
+    b = oracle.OraGraph.load(p).search(z["queries"], meta["k"], meta["ef"])
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    bad = bytearray(v2)
+    bad[len(bad) // 3] ^= 1
+    open(p, "wb").write(bytes(bad))
+    with pytest.raises(IOError):
+        oracle.OraGraph.load(p)
