@@ -138,7 +138,7 @@ int pk_index_prepare_fast(pk_index *h, int traversal);
  * vectors (the returned distances are exact; the ids may differ from the
  * exact search's where low-precision distances reorder the walk).  Arguments
  * as pk_index_search_device; `ef` bounds ef_per_query; expand = list entries
- * expanded per step (1..4, 0 = 1); ef <= 512.  Fully asynchronous on `stream` (no host
+ * expanded per step (1..4, 0 = 1); ef <= 1024.  Fully asynchronous on `stream` (no host
  * synchronisation), so it can be captured in a CUDA graph once buffers have
  * grown to the batch size by an earlier call.  Successive calls on one
  * handle share its scratch: order them on one stream. */
@@ -191,18 +191,18 @@ int pk_index_tune_fast(pk_index *h, const void *queries, int64_t nq, int32_t k, 
                        int32_t *out_shape, float *out_ms, void *stream);
 
 /* Autotuner for batches whose queries carry their own ef: the walk runs one
- * launch per list width (1, 2, 3, 4, 6, 8, 12, 16 slots of 32 entries per
+ * launch per list width (1, 2, 3, 4, 6, 8, 12, 16, 24, 32 slots of 32 entries per
  * lane), and this tunes each width class up to max_ef separately on the given
  * queries (each class at its widest ef, k = min(k, that ef)), keeping one
- * launch shape per class.  out_shapes (8 x 3 ints, may be null) receives
+ * launch shape per class.  out_shapes (10 x 3 ints, may be null) receives
  * rows_per_batch, filter_log2, warps_per_block per class (zeros for classes
- * above max_ef), out_ms (8 floats, may be null) each class's batch time.
+ * above max_ef), out_ms (10 floats, may be null) each class's batch time.
  * pk_index_set_fast_params and pk_index_tune_fast clear the per-class shapes.
  * No counterpart in the reference. */
 int pk_index_tune_fast_classes(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t max_ef,
                                int32_t expand, int32_t *out_shapes, float *out_ms, void *stream);
 
-/* Sets the launch shape of one list-width class (0..7, see above) as
+/* Sets the launch shape of one list-width class (0..9, see above) as
  * pk_index_tune_fast_classes would; all three values 0 = the handle's shape.
  * No counterpart in the reference. */
 int pk_index_set_fast_class_params(pk_index *h, int32_t width_class, int32_t rows_per_batch, int32_t filter_log2,

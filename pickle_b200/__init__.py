@@ -332,12 +332,12 @@ class HNSWIndex:
         """Tune one walk launch shape per list-width class up to max_ef on these
         queries (a torch CUDA tensor), for batches with per-query ef; returns
         {class index: ((rows_per_batch, filter_log2, warps_per_block), ms)}."""
-        shapes = np.zeros(24, np.int32)
-        ms = np.zeros(8, np.float32)
+        shapes = np.zeros(30, np.int32)
+        ms = np.zeros(10, np.float32)
         s = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
         _check(lib().pk_index_tune_fast_classes(self._h, _dev_ptr(queries), queries.shape[0], k, max_ef, expand,
                                                 _ptr(shapes), _ptr(ms), s))
-        return {c: (tuple(int(x) for x in shapes[3 * c:3 * c + 3]), float(ms[c])) for c in range(8)
+        return {c: (tuple(int(x) for x in shapes[3 * c:3 * c + 3]), float(ms[c])) for c in range(10)
                 if shapes[3 * c] > 0}
 
     def set_fast_class_params(self, width_class: int, rows_per_batch: int = 0, filter_log2: int = 0,

@@ -11,8 +11,9 @@
 //   * traversal distances come from a low-precision copy of the vectors,
 //     FP16 or FP8 E4M3 scaled per dimension (a query is scaled by the same
 //     per-dimension factors), as dot products on the tensor cores; for L2
-//     each row carries its stored norm (after its values), which turns the
-//     distance into a dot product;
+//     the row's norm turns the distance into a dot product (E4M3 rows carry
+//     it after their values, FP16 rows get it from the same tensor-core
+//     steps as the Gram diagonal of the staged rows);
 //   * upper layers are descended greedily as in SlideLayer
 //     (include/hnsw.hpp:446-494);
 //   * on layer 0 the result set is a sorted list of ef entries held in
@@ -173,8 +174,8 @@ __device__ __forceinline__ void mma_step(float (&c)[4], const uint32_t (&a)[4], 
 }
 
 // Traversal distances of the n staged rows to the query, into cd[t].  A row's
-// values take data_bytes (whole 32-byte steps); for L2 its stored norm
-// (float) follows them.  All lanes call.
+// values take data_bytes (whole 32-byte steps); for L2 in E4M3 its stored
+// norm (float) follows them.  All lanes call.
 //
 // Sixteen staged rows at a time are the A operand of mma.m16n8k16 (FP16) or
 // mma.m16n8k32 (E4M3): ldmatrix takes one row address per lane, so gathered
@@ -184,7 +185,14 @@ __device__ __forceinline__ void mma_step(float (&c)[4], const uint32_t (&a)[4], 
 // 16 dot products.  E4M3 puts the query's second part (data_bytes into the
 // staged query) in column 1 (lanes 4-7), so one product per k-step yields
 // both; a row's dot product is columns 0 + 1, scaled by qfac.
-// L2 = |q|^2 + |x|^2 - 2 q.x from the stored norms of the same values.
+// L2 = |q|^2 + |x|^2 - 2 q.x.  E4M3 rows carry their norm (per-dimension
+// scales make it no function of the stored codes alone).  FP16 rows are the
+// values divided by one power of two, so |x|^2 in those units is the Gram
+// diagonal of the staged rows: the A fragment registers of rows 0-7 (a[0],
+// a[2]) and of rows 8-15 (a[1], a[3]) are, as they sit, the B fragments of
+// those rows' transposes, and two more products per k-step give A A[0:8]^T
+// and A A[8:16]^T, whose diagonals are the 16 norms - no norm bytes in the
+// row and no extra load.
 template <int TRAV>
 __device__ __forceinline__ void trav_dist_buf(bool ip, float qnorm,
                                               float qfac, const RowFetch &f, int64_t data_bytes, const uint8_t *qbuf,
@@ -193,10 +201,12 @@ __device__ __forceinline__ void trav_dist_buf(bool ip, float qnorm,
     const int ks = (int)(data_bytes / 32);
     const uint32_t *qw = reinterpret_cast<const uint32_t *>(qbuf);
     const int low = (int)(data_bytes / 4);  // E4M3: first word of the query's second part
+    const bool gram = TRAV == kTravF16 && !ip;
     for (int t0 = 0; t0 < n; t0 += 16) {
         const int r = min(t0 + (lane & 15), n - 1);
         const uint32_t arow = smem_u32(f.buf + r * f.stride) + (uint32_t)(lane >> 4) * 16u;
         float c[4] = {0.f, 0.f, 0.f, 0.f};
+        float g0[4] = {0.f, 0.f, 0.f, 0.f}, g1[4] = {0.f, 0.f, 0.f, 0.f};
         for (int kk = 0; kk < ks; kk++) {
             uint32_t a[4];
             asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
@@ -210,15 +220,30 @@ __device__ __forceinline__ void trav_dist_buf(bool ip, float qnorm,
                 b1 = qw[w + 4];
             }
             mma_step<TRAV>(c, a, b0, b1);
+            if (gram) {
+                mma_step<TRAV>(g0, a, a[0], a[2]);
+                mma_step<TRAV>(g1, a, a[1], a[3]);
+            }
         }
-        // columns 0 and 1: lane 4g holds row t0 + g in c[0], c[1] and row
-        // t0 + g + 8 in c[2], c[3]; column 1 is zero for FP16
+        // lane 4g + e of quad g holds columns 2e, 2e + 1 of rows g (c[0],
+        // c[1]) and g + 8 (c[2], c[3]): the query's column 0 is at lane 4g;
+        // the Gram diagonal of row g is column g of g0 (lane 4g + g/2,
+        // element g % 2) and of row g + 8 column g of g1 (same lane, element
+        // 2 + g % 2)
+        const int g = lane >> 2;
+        float na = 0.f, nb = 0.f;
+        if (gram) {
+            const float va = (g & 1) ? g0[1] : g0[0];
+            const float vb = (g & 1) ? g1[3] : g1[2];
+            na = __shfl_sync(kFull, va, 4 * g + (g >> 1));
+            nb = __shfl_sync(kFull, vb, 4 * g + (g >> 1));
+        }
         if ((lane & 3) == 0) {
-            const int ra = t0 + (lane >> 2), rb = ra + 8;
+            const int ra = t0 + g, rb = ra + 8;
             const float da = TRAV == kTravE4M3 ? (c[0] + c[1]) * qfac : c[0];
             const float db = TRAV == kTravE4M3 ? (c[2] + c[3]) * qfac : c[2];
-            if (ra < n) cd[ra] = ip ? -da : qnorm + xnorm(ra) - 2.f * da;
-            if (rb < n) cd[rb] = ip ? -db : qnorm + xnorm(rb) - 2.f * db;
+            if (ra < n) cd[ra] = ip ? -da : qnorm + (gram ? na : xnorm(ra)) - 2.f * da;
+            if (rb < n) cd[rb] = ip ? -db : qnorm + (gram ? nb : xnorm(rb)) - 2.f * db;
         }
     }
     __syncwarp();
@@ -413,13 +438,23 @@ __device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, i
 }
 
 // ------------------------------------------------------------------ walk ---
-// Narrow lists (ef <= 128) fit 80 registers per thread without spills, so
-// three 256-thread blocks can be resident per SM; wider lists take two.
+// Blocks of 256 threads resident per SM that each instantiation is compiled
+// for: three (80 registers per thread, 24 warps per SM) wherever the list and
+// the rest fit 80 registers without spills (ptxas -v): every width up to 4
+// slots, FP16 with one parent per step up to 16 slots (ef <= 512), and
+// otherwise up to 8 slots except FP8 with four parents; two (up to 128
+// registers, 16 warps) for the rest.
+constexpr int walk_min_blocks(int trav, int s, int exp) {
+    return s <= 4 ? 3
+           : (trav == kTravF16 ? (exp == 1 ? s <= 16 : s <= 8) : (exp == 1 && s <= 8)) ? 3
+                                                                                        : 2;
+}
+
 // EXP bounds the parents expanded per step: the walk with one parent per
 // step (the default) has its own instantiation, a quarter of the layer-0
 // loop's code of the one that takes up to four.
 template <int TRAV, int S, int EXP>
-__global__ void __launch_bounds__(256, S <= 4 ? 3 : 2)
+__global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
     walk_kernel(const DevGraph *__restrict__ gp, const WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -755,6 +790,8 @@ void *walk_pick_s(int s) {
         case 8: return (void *)walk_kernel<TRAV, 8, EXP>;
         case 12: return (void *)walk_kernel<TRAV, 12, EXP>;
         case 16: return (void *)walk_kernel<TRAV, 16, EXP>;
+        case 24: return (void *)walk_kernel<TRAV, 24, EXP>;
+        case 32: return (void *)walk_kernel<TRAV, 32, EXP>;
         default: return nullptr;
     }
 }

@@ -8,7 +8,7 @@ namespace pk {
 constexpr int kTravF16 = 1;   // traversal copy in FP16
 constexpr int kTravE4M3 = 2;  // traversal copy in FP8 E4M3 with per-dimension scales
 
-constexpr int kFastMaxEf = 512;  // the walk's register list holds up to 32 * 16 entries
+constexpr int kFastMaxEf = 1024;  // the walk's register list holds up to 32 * 32 entries
 
 // Bytes of a traversal query row: FP16 = the values; E4M3 = the query's two
 // E4M3 parts and a 16-byte chunk holding its power-of-two factor.
@@ -40,7 +40,7 @@ struct WalkArgs {
     const uint8_t *trav_zero;   // a zero row of the traversal copy
     int64_t trav_row_bytes;
     int64_t trav_rows;          // rows in the traversal copy; node ids stay below it
-    int64_t trav_data_bytes;    // the values of a row; for L2 the row's norm follows them (float)
+    int64_t trav_data_bytes;    // the values of a row; E4M3 L2 rows have their norm after them (float)
 };
 
 // Shared-memory stride of a staged traversal row: the row padded to an odd
@@ -126,9 +126,9 @@ __host__ __device__ inline RerankLayout rerank_layout(int cand_stride, int64_t r
 // List widths: slots per lane of the register list, which holds 32 entries
 // per slot.  A query takes the narrowest width that holds its ef, so its list
 // is at most twice ef (ef <= 64) or half again as wide (ef > 64).
-constexpr int kSlotClasses = 8;
-__host__ __device__ inline int slot_class_width(int c) {
-    return c < 3 ? c + 1 : c == 3 ? 4 : c == 4 ? 6 : c == 5 ? 8 : c == 6 ? 12 : 16;  // 1 2 3 4 6 8 12 16
+constexpr int kSlotClasses = 10;
+__host__ __device__ inline int slot_class_width(int c) {  // 1 2 3 4 6 8 12 16 24 32
+    return c < 3 ? c + 1 : c == 3 ? 4 : c == 4 ? 6 : c == 5 ? 8 : c == 6 ? 12 : c == 7 ? 16 : c == 8 ? 24 : 32;
 }
 __host__ __device__ inline int slot_class(int ef) {
     int c = 0;

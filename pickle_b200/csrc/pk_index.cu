@@ -165,7 +165,7 @@ struct pk_index {
     // low-precision traversal copy and the fast path's scratch
     int trav = 0;                  // 0 none, pk::kTravF16, pk::kTravE4M3
     int64_t trav_row_bytes = 0, trav_rows = 0, trav_cap = 0;
-    int64_t trav_data_bytes = 0;   // the traversal values; L2 rows add a 16-byte chunk with the row's norm
+    int64_t trav_data_bytes = 0;   // the traversal values; E4M3 L2 rows add a 32-byte chunk with the row's norm
     uint8_t *d_trav = nullptr, *d_trav_zero = nullptr;
     float *d_scale = nullptr, *d_rownorm = nullptr;
     float trav_f16_scale = 1.0f;   // FP16 copy = vectors / this power of two
@@ -754,11 +754,14 @@ float f16_scale(const std::vector<float> &m) {
 int build_traversal(pk_index *h, int trav) {
     cudaStream_t s = h->stream;
     // values padded with zeros to whole 32-byte steps of the tensor-core dot
-    // products (16 FP16 or 32 E4M3 elements); for L2 a 32-byte chunk after
-    // them holds the row's sum of squares, so a row's bulk copy brings its
-    // norm along and rows stay on whole 32-byte sectors
+    // products (16 FP16 or 32 E4M3 elements); for L2 in E4M3 a 32-byte chunk
+    // after them holds the row's sum of squares (in original units, which the
+    // per-dimension scales keep from being a function of the codes), so a
+    // row's bulk copy brings its norm along and rows stay on whole 32-byte
+    // sectors.  FP16 rows need no norm: the walk takes it from the Gram
+    // diagonal of the staged rows.
     const int64_t tdb = trav == pk::kTravF16 ? (h->dim * 2 + 31) / 32 * 32 : (h->dim + 31) / 32 * 32;
-    const int64_t trb = tdb + (h->metric == PK_METRIC_L2 ? 32 : 0);
+    const int64_t trb = tdb + (h->metric == PK_METRIC_L2 && trav == pk::kTravE4M3 ? 32 : 0);
     const int64_t rows = std::max<int64_t>(h->vec_rows, 1);
     PK_CUDA(cudaStreamSynchronize(s));
     dfree(h, h->d_trav, (size_t)(h->trav_cap * h->trav_row_bytes));
@@ -787,7 +790,7 @@ int build_traversal(pk_index *h, int trav) {
     }
     PK_CUDA(cudaMemcpyAsync(h->d_scale, scale.data(), 4 * (size_t)h->dim, cudaMemcpyHostToDevice, s));
     PK_CUDA(pk::launch_convert_rows(h->dtype, trav, h->hg.vec0, h->row_bytes, 0, h->n0(), (int)h->dim, h->d_scale,
-                                    h->d_trav, trb, h->metric == PK_METRIC_L2 ? tdb : -1, h->d_rownorm, s));
+                                    h->d_trav, trb, trb > tdb ? tdb : -1, h->d_rownorm, s));
     PK_CUDA(cudaStreamSynchronize(s));
     h->trav = trav;
     h->trav_row_bytes = trb;
@@ -812,7 +815,8 @@ int refresh_traversal(pk_index *h) {
     }
     PK_CUDA(pk::launch_convert_rows(h->dtype, h->trav, h->hg.vec0, h->row_bytes, h->trav_rows, h->n0(), (int)h->dim,
                                     h->d_scale, h->d_trav, h->trav_row_bytes,
-                                    h->metric == PK_METRIC_L2 ? h->trav_data_bytes : -1, h->d_rownorm, h->stream));
+                                    h->trav_row_bytes > h->trav_data_bytes ? h->trav_data_bytes : -1, h->d_rownorm,
+                                    h->stream));
     PK_CUDA(cudaStreamSynchronize(h->stream));
     h->trav_rows = h->n0();
     return PK_OK;
@@ -854,7 +858,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
                     int32_t ef, const int32_t *k_arr, const int32_t *ef_arr, int32_t stride, int32_t *ids,
                     float *dists, int32_t *counters, int32_t expand, cudaStream_t s) {
     if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
-    if (ef > pk::kFastMaxEf) return fail(PK_ERR_ARG, "ef too large for the fast path (max 512)");
+    if (ef > pk::kFastMaxEf) return fail(PK_ERR_ARG, "ef too large for the fast path (max 1024)");
     PK_TRY(refresh_traversal(h));
     const int slots = pk::list_slots(ef);
     const int cs = 32 * slots;
@@ -2206,7 +2210,7 @@ int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter
 int pk_index_set_fast_class_params(pk_index *h, int32_t width_class, int32_t rows_per_batch, int32_t filter_log2,
                                    int32_t warps_per_block) {
     if (!h) return fail(PK_ERR_ARG, "NULL handle");
-    if (width_class < 0 || width_class >= pk::kSlotClasses) return fail(PK_ERR_ARG, "width_class must be 0..7");
+    if (width_class < 0 || width_class >= pk::kSlotClasses) return fail(PK_ERR_ARG, "width_class must be 0..9");
     if (rows_per_batch < 0 || rows_per_batch > 256) return fail(PK_ERR_ARG, "rows_per_batch must be 0..256");
     if (filter_log2 != 0 && (filter_log2 < 5 || filter_log2 > 15))
         return fail(PK_ERR_ARG, "filter_log2 must be 0 or 5..15");
