@@ -210,19 +210,27 @@ int pk_index_set_fast_class_params(pk_index *h, int32_t width_class, int32_t row
 
 /* Serving: continuous batching over pk_index_search_fast.  No counterpart
  * in the reference (its batch AnnSearch is a blocking OpenMP loop,
- * include/hnsw.hpp:528-541).  A worker thread owns `slots` execution slots,
- * each with its own stream, scratch and buffers for max_batch queries
- * (allocated at creation: device memory is fixed, admission is by slot and
- * batch capacity).  Submitted requests (nq queries sharing one k <= max_k and
- * one ef <= max_ef) wait in FIFO order and are packed into whichever slot frees
- * up first; slots in flight overlap on the GPU.  Each result equals what
- * pk_index_search_fast returns for that request alone.  A slot that does not
+ * include/hnsw.hpp:528-541).  A worker thread owns `slots` streams and one
+ * arena of device memory.  Submitted requests (nq queries sharing one
+ * k <= max_k and one ef <= max_ef <= 1024) wait in FIFO order; whenever a
+ * stream is free, queued requests are packed into a batch of up to max_batch
+ * queries for as long as the batch's device buffers - sized from the batch's
+ * own query count, largest k and largest ef (pk_server_request_bytes gives a
+ * request's share) - fit the arena's free space; batches in flight overlap on
+ * the GPU and give their memory back when they finish.  Admission is thus by
+ * device memory: a request that does not fit waits (deferred for memory, see
+ * pk_server_memory) even while streams are free, and one larger than the
+ * whole arena is refused at submission with PK_ERR_CAPACITY.  The arena is
+ * device_bytes (pk_server_create_with_memory) or, for pk_server_create, enough
+ * for every stream's full batch at max_k and max_ef but at most half of the
+ * device memory free at creation.  Each result equals what
+ * pk_index_search_fast returns for that request alone.  A batch that does not
  * finish within the watchdog period (30 s) fails its requests with
  * PK_ERR_TIMEOUT.  The index must not be modified while a server uses it.
  * submit copies the queries and returns a ticket at once; wait blocks until
  * the ticket's results are ready (timeout_ms < 0: no limit), copies nq*k ids
  * and distances out, and reports the latency from submit to completion.
- * stats: out[0..4] = batches launched, queries served, most slots in flight
+ * stats: out[0..4] = batches launched, queries served, most batches in flight
  * at once, requests queued, error status. */
 typedef struct pk_server pk_server;
 int pk_server_create(pk_server **out, pk_index *h, int traversal, int slots, int32_t max_batch, int32_t max_k,
@@ -231,6 +239,14 @@ int pk_server_submit(pk_server *s, const void *queries, int32_t nq, int32_t k, i
 int pk_server_wait(pk_server *s, int64_t ticket, int32_t *out_ids, float *out_dists, double *latency_ms,
                    int32_t timeout_ms);
 int pk_server_stats(pk_server *s, int64_t *out);
+int pk_server_create_with_memory(pk_server **out, pk_index *h, int traversal, int slots, int32_t max_batch,
+                                 int32_t max_k, int32_t max_ef, int32_t expand, int64_t device_bytes);
+/* out[0..3] = arena bytes, bytes in use now, most bytes in use at once,
+ * requests that had to wait for device memory. */
+int pk_server_memory(pk_server *s, int64_t *out);
+/* Device bytes a request of nq queries at k and ef takes while it runs (the
+ * share admission checks against the arena). */
+int pk_server_request_bytes(pk_server *s, int32_t nq, int32_t k, int32_t ef, int64_t *bytes);
 /* Replays a timed request trace through the server: request i (nq[i]
  * consecutive rows of `queries`, k[i], ef[i]) is submitted arrival_us[i]
  * microseconds after the call starts, by a producer thread that waits for each

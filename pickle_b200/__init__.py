@@ -85,6 +85,9 @@ def lib() -> ctypes.CDLL:
         L.pk_server_set_watchdog.argtypes = [P, ctypes.c_double]
         L.pk_server_destroy.argtypes = [P]
         L.pk_server_replay.argtypes = [P, VP, I64, VP, VP, VP, VP, VP, VP, I32, VP]
+        L.pk_server_create_with_memory.argtypes = [PP, P, ctypes.c_int, ctypes.c_int, I32, I32, I32, I32, I64]
+        L.pk_server_memory.argtypes = [P, VP]
+        L.pk_server_request_bytes.argtypes = [P, I32, I32, I32, ctypes.POINTER(ctypes.c_int64)]
         for name in ["pk_index_create", "pk_index_destroy", "pk_index_set_seed", "pk_index_set_levels",
                      "pk_index_build", "pk_index_add", "pk_index_search", "pk_index_search_device",
                      "pk_index_save", "pk_index_load", "pk_index_info", "pk_index_layer", "pk_index_prepare_fast",
@@ -92,7 +95,8 @@ def lib() -> ctypes.CDLL:
                      "pk_index_search_var", "pk_index_search_fast_host_var", "pk_index_tune_fast_classes",
                      "pk_index_set_fast_class_params",
                      "pk_server_create", "pk_server_submit", "pk_server_wait", "pk_server_stats",
-                     "pk_server_set_watchdog", "pk_server_destroy", "pk_server_replay"]:
+                     "pk_server_set_watchdog", "pk_server_destroy", "pk_server_replay",
+                     "pk_server_create_with_memory", "pk_server_memory", "pk_server_request_bytes"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -435,19 +439,32 @@ class HNSWIndex:
 class Server:
     """Continuous-batching search server over an index (pk_server_* in the C ABI).
 
-    Server(index, traversal="f16", slots=4, max_batch=4096, max_k=100, max_ef=256)
+    Server(index, traversal="f16", slots=4, max_batch=4096, max_k=100, max_ef=256, device_bytes=0)
     submit(queries, k, ef) -> ticket (returns at once); wait(ticket) -> (ids, dists, latency_ms).
+    Batches are admitted by device memory: device_bytes is the server's arena
+    (0 = every slot's full batch at max_k and max_ef, at most half the free
+    device memory); memory() reports its use and the requests that waited.
     """
 
     def __init__(self, index: "HNSWIndex", traversal: str = "f16", slots: int = 4, max_batch: int = 4096,
-                 max_k: int = 100, max_ef: int = 256, expand: int = 1):
+                 max_k: int = 100, max_ef: int = 256, expand: int = 1, device_bytes: int = 0):
         self.index = index
         self._s = None
         s = ctypes.c_void_p()
-        _check(lib().pk_server_create(ctypes.byref(s), index._h, HNSWIndex.TRAVERSAL[traversal], slots, max_batch,
-                                      max_k, max_ef, expand))
+        _check(lib().pk_server_create_with_memory(ctypes.byref(s), index._h, HNSWIndex.TRAVERSAL[traversal], slots,
+                                                  max_batch, max_k, max_ef, expand, device_bytes))
         self._s = s
         self._shape = {}
+
+    def memory(self) -> dict:
+        out = np.zeros(4, np.int64)
+        _check(lib().pk_server_memory(self._s, _ptr(out)))
+        return dict(zip(["arena_bytes", "in_use", "peak_in_use", "deferred_for_memory"], (int(x) for x in out)))
+
+    def request_bytes(self, nq: int, k: int, ef: int) -> int:
+        b = ctypes.c_int64()
+        _check(lib().pk_server_request_bytes(self._s, nq, k, ef, ctypes.byref(b)))
+        return b.value
 
     def submit(self, queries: np.ndarray, k: int, ef: int) -> int:
         q = self.index._rows(queries)

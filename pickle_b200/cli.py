@@ -115,8 +115,7 @@ def cmd_gen(a):
         x, q = datasets.gmm_f16(a.n or 10_000_000, a.nq or 100_000, 128, ncomp=1024, sigma=0.5, seed=a.seed)
         metric = "l2"
     elif a.config == "c5":
-        x, q = datasets.gmm_unit(a.n or 5_000_000, a.nq or 10_000, 768, ncomp=2048, sigma=0.3, seed=a.seed,
-                                 dtype=np.float16, zipf_s=1.1)
+        x, q = datasets.embedding_like(a.n or 5_000_000, a.nq or 10_000, 768, ncomp=2048, zipf_s=1.1, seed=a.seed)
         metric = "ip"
     else:
         raise SystemExit(f"unknown config {a.config}")

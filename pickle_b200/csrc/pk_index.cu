@@ -1651,16 +1651,20 @@ static int pk_index_search_fast_host_var_impl(pk_index *h, const void *queries, 
 
 // ---------------------------------------------------------------- server ----
 // Continuous batching over the fast search.  A worker thread owns `slots`
-// execution slots; each has its own stream, scratch (FastCtx), pinned host
-// staging and device buffers sized for max_batch queries.  Requests (each a
-// group of queries with one k and ef) wait in a FIFO; whenever a slot is free,
-// the worker packs queued requests into it up to max_batch queries, copies
-// them in, launches the search with per-query k and ef, copies the results
-// out and records an event.  Slots in flight overlap on the device; a slot is
-// refilled as soon as its event completes.  Device memory is fixed at creation
-// (admission is by slot and batch capacity); a slot whose work has not
-// completed within the watchdog period fails its requests with
-// PK_ERR_TIMEOUT.
+// execution streams.  Requests (each a group of queries with one k and ef)
+// wait in a FIFO; whenever a stream is free, the worker packs queued
+// requests into a batch of up to max_batch queries as long as the batch's
+// device buffers (queries, per-query k and ef, results, the walk's scratch,
+// all sized from the batch's own nq, largest k and largest ef) fit the free
+// part of the server's device-memory arena, carves them out of it, copies the
+// batch in, launches the search with per-query k and ef, copies the results
+// out and records an event.  Batches in flight overlap on the device; a
+// finished batch returns its memory and its stream.  So the number of
+// queries in flight follows the memory their k and ef need: many small
+// requests run side by side, a large one waits until enough is free (counted
+// as deferred for memory), and one larger than the whole arena is refused at
+// submission.  A batch that has not completed within the watchdog period
+// fails its requests with PK_ERR_TIMEOUT.
 namespace {
 
 using Clock = std::chrono::steady_clock;
@@ -1674,23 +1678,28 @@ struct SrvRequest {
     Clock::time_point t_submit, t_done;
     int status = 0;
     bool done = false;
+    bool deferred = false;  // once found waiting for device memory
+};
+
+// Where a batch's device buffers sit in the server's arena (byte offsets).
+struct SrvLayout {
+    size_t q = 0, k = 0, ef = 0, ids = 0, d = 0, work = 0, cand = 0, lists = 0, fq = 0, tq = 0, qn = 0, total = 0;
+    int64_t cand_n = 0, lists_n = 0, fq_n = 0, tq_n = 0, qn_n = 0;
 };
 
 struct SrvSlot {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
-    FastCtx ctx;
+    FastCtx ctx;                   // points into the arena while a batch runs
     uint8_t *h_q = nullptr;
     int32_t *h_k = nullptr, *h_ef = nullptr, *h_ids = nullptr;
     float *h_d = nullptr;
-    uint8_t *d_q = nullptr;
-    int32_t *d_k = nullptr, *d_ef = nullptr, *d_ids = nullptr;
-    float *d_d = nullptr;
     int32_t *h_status = nullptr;   // the walk's status, copied back with the results
     bool busy = false;
     std::vector<std::shared_ptr<SrvRequest>> reqs;
     std::vector<int32_t> offs;
-    int32_t nq = 0;
+    int32_t nq = 0, stride = 0;
+    size_t chunk_off = 0, chunk_bytes = 0;  // the batch's arena chunk
     Clock::time_point t_launch;
 };
 
@@ -1701,6 +1710,12 @@ struct pk_server {
     int32_t max_batch = 0, max_k = 0, max_ef = 0, expand = 1;
     double watchdog_s = 30.0;
     std::vector<SrvSlot> slots;
+    // device memory: one arena, carved per batch (first fit); admission waits
+    // while the queue's next request does not fit the free space
+    uint8_t *arena = nullptr;
+    size_t arena_bytes = 0, in_use = 0, peak_in_use = 0;
+    std::vector<std::pair<size_t, size_t>> free_list;  // (offset, bytes), sorted by offset
+    int64_t deferred_for_memory = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<std::shared_ptr<SrvRequest>> queue;
@@ -1715,6 +1730,80 @@ struct pk_server {
 
 namespace {
 
+// Device bytes of a batch of nq queries whose largest k and ef are kmax and
+// efmax: the server's copies of queries, k, ef and results, and what the
+// fast search needs for them (pk_index_search_fast's scratch).
+SrvLayout srv_layout(const pk_index *h, int64_t nq, int32_t kmax, int32_t efmax) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    SrvLayout L;
+    const size_t w = (size_t)(h->dim * h->esz);
+    const int64_t cs = 32 * pk::list_slots(std::min(efmax, pk::kFastMaxEf));
+    const int64_t tq_rb = pk::trav_query_bytes(h->trav, h->trav_data_bytes);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = off;
+        off += al(std::max<size_t>(bytes, 16));
+        return at;
+    };
+    L.q = take(nq * w);
+    L.k = take(4 * nq);
+    L.ef = take(4 * nq);
+    L.ids = take(4 * nq * kmax);
+    L.d = take(4 * nq * kmax);
+    L.work = take(4 * (size_t)kWorkInts);
+    L.cand_n = nq * cs;
+    L.cand = take(4 * L.cand_n);
+    L.lists_n = nq * pk::kSlotClasses;
+    L.lists = take(4 * L.lists_n);
+    L.fq_n = w != (size_t)h->row_bytes ? nq * h->row_bytes : 0;
+    L.fq = take((size_t)L.fq_n);
+    L.tq_n = nq * tq_rb;
+    L.tq = take((size_t)L.tq_n);
+    L.qn_n = nq;
+    L.qn = take(4 * nq);
+    L.total = off;
+    return L;
+}
+
+// First fit in the arena (caller holds S->mu); false if nothing fits.
+bool arena_take(pk_server *S, size_t bytes, size_t &off) {
+    for (size_t i = 0; i < S->free_list.size(); i++) {
+        auto &f = S->free_list[i];
+        if (f.second < bytes) continue;
+        off = f.first;
+        f.first += bytes;
+        f.second -= bytes;
+        if (f.second == 0) S->free_list.erase(S->free_list.begin() + (long)i);
+        S->in_use += bytes;
+        S->peak_in_use = std::max(S->peak_in_use, S->in_use);
+        return true;
+    }
+    return false;
+}
+
+size_t arena_largest(const pk_server *S) {
+    size_t m = 0;
+    for (const auto &f : S->free_list) m = std::max(m, f.second);
+    return m;
+}
+
+void arena_give(pk_server *S, size_t off, size_t bytes) {
+    if (bytes == 0) return;
+    auto &fl = S->free_list;
+    auto it = std::lower_bound(fl.begin(), fl.end(), std::make_pair(off, (size_t)0));
+    it = fl.insert(it, {off, bytes});
+    // merge with the neighbours
+    if (it + 1 != fl.end() && it->first + it->second == (it + 1)->first) {
+        it->second += (it + 1)->second;
+        fl.erase(it + 1);
+    }
+    if (it != fl.begin() && (it - 1)->first + (it - 1)->second == it->first) {
+        (it - 1)->second += it->second;
+        fl.erase(it);
+    }
+    S->in_use -= std::min(S->in_use, bytes);
+}
+
 void srv_fail_all(pk_server *S, int code) {
     // caller holds S->mu
     S->error = code;
@@ -1727,6 +1816,15 @@ void srv_fail_all(pk_server *S, int code) {
     S->cv_done.notify_all();
 }
 
+void srv_finish_slot(pk_server *S, SrvSlot &sl) {
+    // caller holds S->mu
+    arena_give(S, sl.chunk_off, sl.chunk_bytes);
+    sl.chunk_bytes = 0;
+    sl.reqs.clear();
+    sl.offs.clear();
+    sl.busy = false;
+}
+
 void srv_loop(pk_server *S) {
     pk_index *h = S->h;
     cudaSetDevice(h->device);
@@ -1736,7 +1834,7 @@ void srv_loop(pk_server *S) {
         // 1. completions
         for (SrvSlot &sl : S->slots) {
             if (!sl.busy) continue;
-            // the watchdog looks first: a slot whose completion the host has
+            // the watchdog looks first: a batch whose completion the host has
             // not observed within the period fails, finished or not
             double wd;
             {
@@ -1750,6 +1848,8 @@ void srv_loop(pk_server *S) {
                     r->done = true;
                     r->t_done = Clock::now();
                 }
+                // the batch may still be running: its memory stays taken
+                sl.chunk_bytes = 0;
                 sl.reqs.clear();
                 sl.offs.clear();
                 srv_fail_all(S, PK_ERR_TIMEOUT);
@@ -1770,21 +1870,19 @@ void srv_loop(pk_server *S) {
                     r.dists.resize((size_t)r.nq * r.k);
                     for (int32_t j = 0; j < r.nq; j++) {
                         const int64_t row = sl.offs[i] + j;
-                        std::memcpy(r.ids.data() + (size_t)j * r.k, sl.h_ids + row * S->max_k, 4 * (size_t)r.k);
-                        std::memcpy(r.dists.data() + (size_t)j * r.k, sl.h_d + row * S->max_k, 4 * (size_t)r.k);
+                        std::memcpy(r.ids.data() + (size_t)j * r.k, sl.h_ids + row * sl.stride, 4 * (size_t)r.k);
+                        std::memcpy(r.dists.data() + (size_t)j * r.k, sl.h_d + row * sl.stride, 4 * (size_t)r.k);
                     }
                 }
                 r.done = true;
                 r.t_done = now;
             }
             if (code != PK_OK) srv_fail_all(S, code);
-            sl.reqs.clear();
-            sl.offs.clear();
-            sl.busy = false;
+            srv_finish_slot(S, sl);
             did = true;
             S->cv_done.notify_all();
         }
-        // 2. admissions into free slots
+        // 2. admissions into free streams, as far as the arena has room
         {
             std::unique_lock<std::mutex> lk(S->mu);
             if (S->stop) break;
@@ -1792,34 +1890,79 @@ void srv_loop(pk_server *S) {
             for (SrvSlot &sl : S->slots) inflight += sl.busy;
             for (SrvSlot &sl : S->slots) {
                 if (sl.busy || S->queue.empty() || S->error) continue;
-                int32_t nq = 0;
-                while (!S->queue.empty() && nq + S->queue.front()->nq <= S->max_batch) {
+                const size_t room = arena_largest(S);
+                int32_t nq = 0, kmax = 0, efmax = 0;
+                size_t need = 0, count = 0;
+                for (const auto &r : S->queue) {
+                    if (nq + r->nq > S->max_batch) break;
+                    const SrvLayout L = srv_layout(h, nq + r->nq, std::max(kmax, r->k), std::max(efmax, r->ef));
+                    if (L.total > room) break;
+                    nq += r->nq;
+                    kmax = std::max(kmax, r->k);
+                    efmax = std::max(efmax, r->ef);
+                    need = L.total;
+                    count++;
+                }
+                if (count == 0) {
+                    // the head waits for device memory, not for a stream
+                    if (!S->queue.front()->deferred) {
+                        S->queue.front()->deferred = true;
+                        S->deferred_for_memory++;
+                    }
+                    break;
+                }
+                size_t off = 0;
+                if (!arena_take(S, need, off)) break;
+                const SrvLayout L = srv_layout(h, nq, kmax, efmax);
+                sl.chunk_off = off;
+                sl.chunk_bytes = need;
+                sl.stride = kmax;
+                int32_t at = 0;
+                for (size_t i = 0; i < count; i++) {
                     auto r = S->queue.front();
                     S->queue.pop_front();
-                    sl.offs.push_back(nq);
-                    std::memcpy(sl.h_q + (size_t)nq * w, r->q.data(), (size_t)r->nq * w);
+                    sl.offs.push_back(at);
+                    std::memcpy(sl.h_q + (size_t)at * w, r->q.data(), (size_t)r->nq * w);
                     for (int32_t j = 0; j < r->nq; j++) {
-                        sl.h_k[nq + j] = r->k;
-                        sl.h_ef[nq + j] = r->ef;
+                        sl.h_k[at + j] = r->k;
+                        sl.h_ef[at + j] = r->ef;
                     }
-                    nq += r->nq;
+                    at += r->nq;
                     sl.reqs.push_back(std::move(r));
                 }
-                if (nq == 0) continue;
                 sl.nq = nq;
+                uint8_t *base = S->arena + off;
+                uint8_t *d_q = base + L.q;
+                int32_t *d_k = reinterpret_cast<int32_t *>(base + L.k);
+                int32_t *d_ef = reinterpret_cast<int32_t *>(base + L.ef);
+                int32_t *d_ids = reinterpret_cast<int32_t *>(base + L.ids);
+                float *d_d = reinterpret_cast<float *>(base + L.d);
+                // the search's scratch, in the chunk (sized so that nothing grows)
+                sl.ctx.d_work = reinterpret_cast<int32_t *>(base + L.work);
+                sl.ctx.work_n = kWorkInts;
+                sl.ctx.d_cand = reinterpret_cast<int32_t *>(base + L.cand);
+                sl.ctx.cand_n = L.cand_n;
+                sl.ctx.d_lists = reinterpret_cast<int32_t *>(base + L.lists);
+                sl.ctx.lists_n = L.lists_n;
+                sl.ctx.d_fq = L.fq_n ? base + L.fq : nullptr;
+                sl.ctx.fq_n = L.fq_n;
+                sl.ctx.d_tq = base + L.tq;
+                sl.ctx.tq_n = L.tq_n;
+                sl.ctx.d_qn = reinterpret_cast<float *>(base + L.qn);
+                sl.ctx.qn_n = L.qn_n;
                 lk.unlock();
                 int rc = PK_OK;
-                if (cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)nq * w, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
-                    cudaMemcpyAsync(sl.d_k, sl.h_k, 4 * (size_t)nq, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
-                    cudaMemcpyAsync(sl.d_ef, sl.h_ef, 4 * (size_t)nq, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess)
+                if (cudaMemcpyAsync(d_q, sl.h_q, (size_t)nq * w, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
+                    cudaMemcpyAsync(d_k, sl.h_k, 4 * (size_t)nq, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess ||
+                    cudaMemcpyAsync(d_ef, sl.h_ef, 4 * (size_t)nq, cudaMemcpyHostToDevice, sl.stream) != cudaSuccess)
                     rc = PK_ERR_CUDA;
                 if (rc == PK_OK)
-                    rc = run_search_fast(h, sl.ctx, sl.d_q, false, nq, S->max_k, S->max_ef, sl.d_k, sl.d_ef, S->max_k,
-                                         sl.d_ids, sl.d_d, nullptr, S->expand, sl.stream);
+                    rc = run_search_fast(h, sl.ctx, d_q, false, nq, kmax, efmax, d_k, d_ef, kmax, d_ids, d_d, nullptr,
+                                         S->expand, sl.stream);
                 if (rc == PK_OK &&
-                    (cudaMemcpyAsync(sl.h_ids, sl.d_ids, 4 * (size_t)nq * S->max_k, cudaMemcpyDeviceToHost,
-                                     sl.stream) != cudaSuccess ||
-                     cudaMemcpyAsync(sl.h_d, sl.d_d, 4 * (size_t)nq * S->max_k, cudaMemcpyDeviceToHost, sl.stream) !=
+                    (cudaMemcpyAsync(sl.h_ids, d_ids, 4 * (size_t)nq * kmax, cudaMemcpyDeviceToHost, sl.stream) !=
+                         cudaSuccess ||
+                     cudaMemcpyAsync(sl.h_d, d_d, 4 * (size_t)nq * kmax, cudaMemcpyDeviceToHost, sl.stream) !=
                          cudaSuccess ||
                      cudaMemcpyAsync(sl.h_status, sl.ctx.d_work + kWorkStatus, sizeof(int32_t), cudaMemcpyDeviceToHost,
                                      sl.stream) != cudaSuccess ||
@@ -1832,8 +1975,8 @@ void srv_loop(pk_server *S) {
                         r->done = true;
                         r->t_done = Clock::now();
                     }
-                    sl.reqs.clear();
-                    sl.offs.clear();
+                    cudaStreamSynchronize(sl.stream);
+                    srv_finish_slot(S, sl);
                     srv_fail_all(S, rc);
                     continue;
                 }
@@ -1862,33 +2005,34 @@ void srv_loop(pk_server *S) {
 void srv_free(pk_server *S) {
     for (SrvSlot &sl : S->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
-        free_fast_ctx(S->h, sl.ctx);
+        // the slot's scratch lives in the arena: only its events are its own
+        for (cudaEvent_t &e : sl.ctx.ev)
+            if (e) cudaEventDestroy(e);
         cudaFreeHost(sl.h_q);
         cudaFreeHost(sl.h_k);
         cudaFreeHost(sl.h_ef);
         cudaFreeHost(sl.h_ids);
         cudaFreeHost(sl.h_d);
         cudaFreeHost(sl.h_status);
-        cudaFree(sl.d_q);
-        cudaFree(sl.d_k);
-        cudaFree(sl.d_ef);
-        cudaFree(sl.d_ids);
-        cudaFree(sl.d_d);
         if (sl.ev) cudaEventDestroy(sl.ev);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
+    if (S->arena) dfree(S->h, S->arena, S->arena_bytes);
     delete S;
 }
 
 int srv_create(pk_server **out, pk_index *h, int traversal, int nslots, int32_t max_batch, int32_t max_k,
-               int32_t max_ef, int32_t expand) {
-    if (!out || !h || nslots < 1 || nslots > 64 || max_batch < 1 || max_k < 1 || max_ef < max_k)
-        return fail(PK_ERR_ARG, "bad server arguments (need 1 <= slots <= 64, max_batch >= 1, max_ef >= max_k >= 1)");
+               int32_t max_ef, int32_t expand, int64_t device_bytes) {
+    if (!out || !h || nslots < 1 || nslots > 64 || max_batch < 1 || max_k < 1 || max_ef < max_k ||
+        max_ef > pk::kFastMaxEf || device_bytes < 0)
+        return fail(PK_ERR_ARG, "bad server arguments (need 1 <= slots <= 64, max_batch >= 1, "
+                                "1 <= max_k <= max_ef <= 1024, device_bytes >= 0)");
     if (h->n0() == 0) return fail(PK_ERR_STATE, "the index is empty");
     if (h->trav != (traversal == PK_TRAVERSAL_F16 ? pk::kTravF16 : pk::kTravE4M3)) {
         int rc = pk_index_prepare_fast_impl(h, traversal);
         if (rc != PK_OK) return rc;
     }
+    PK_TRY(refresh_traversal(h));
     auto *S = new (std::nothrow) pk_server();
     if (!S) return fail(PK_ERR_OOM, "host allocation failed");
     S->h = h;
@@ -1896,6 +2040,25 @@ int srv_create(pk_server **out, pk_index *h, int traversal, int nslots, int32_t 
     S->max_k = max_k;
     S->max_ef = max_ef;
     S->expand = std::max(1, expand);
+    // the arena: as asked, else every stream's full batch at the largest k
+    // and ef, but at most half of the device memory free now
+    size_t bytes = (size_t)device_bytes;
+    if (bytes == 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            delete S;
+            return fail(PK_ERR_CUDA, "cudaMemGetInfo failed");
+        }
+        bytes = std::min(srv_layout(h, max_batch, max_k, max_ef).total * (size_t)nslots, fr / 2);
+    }
+    bytes = (bytes + 255) & ~(size_t)255;
+    if (dalloc(h, (void **)&S->arena, bytes) != PK_OK) {
+        delete S;
+        return fail(PK_ERR_OOM, "the server's device memory (" + std::to_string(bytes) + " bytes) is not free");
+    }
+    S->arena_bytes = bytes;
+    S->free_list.push_back({0, bytes});
     S->slots.resize(nslots);
     const size_t w = (size_t)(h->dim * h->esz);
     for (SrvSlot &sl : S->slots) {
@@ -1906,35 +2069,10 @@ int srv_create(pk_server **out, pk_index *h, int traversal, int nslots, int32_t 
             cudaMallocHost((void **)&sl.h_ef, 4 * (size_t)max_batch) != cudaSuccess ||
             cudaMallocHost((void **)&sl.h_ids, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
             cudaMallocHost((void **)&sl.h_d, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
-            cudaMallocHost((void **)&sl.h_status, sizeof(int32_t)) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_q, (size_t)max_batch * w) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_k, 4 * (size_t)max_batch) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_ef, 4 * (size_t)max_batch) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_ids, 4 * (size_t)max_batch * max_k) != cudaSuccess ||
-            cudaMalloc((void **)&sl.d_d, 4 * (size_t)max_batch * max_k) != cudaSuccess) {
+            cudaMallocHost((void **)&sl.h_status, sizeof(int32_t)) != cudaSuccess) {
             cudaGetLastError();
             srv_free(S);
-            return fail(PK_ERR_OOM, "server buffers could not be allocated");
-        }
-        // grow this slot's scratch to the full batch now, so that serving
-        // allocates nothing: one search of max_batch zero queries
-        std::memset(sl.h_q, 0, (size_t)max_batch * w);
-        for (int32_t i = 0; i < max_batch; i++) {
-            sl.h_k[i] = max_k;
-            sl.h_ef[i] = max_ef;
-        }
-        int rc = PK_OK;
-        if (cudaMemcpy(sl.d_q, sl.h_q, (size_t)max_batch * w, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(sl.d_k, sl.h_k, 4 * (size_t)max_batch, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(sl.d_ef, sl.h_ef, 4 * (size_t)max_batch, cudaMemcpyHostToDevice) != cudaSuccess)
-            rc = fail(PK_ERR_CUDA, "server warm-up copy failed");
-        if (rc == PK_OK)
-            rc = run_search_fast(h, sl.ctx, sl.d_q, false, max_batch, max_k, max_ef, sl.d_k, sl.d_ef, max_k, sl.d_ids,
-                                 sl.d_d, nullptr, S->expand, sl.stream);
-        if (rc == PK_OK && cudaStreamSynchronize(sl.stream) != cudaSuccess) rc = fail(PK_ERR_CUDA, "warm-up failed");
-        if (rc != PK_OK) {
-            srv_free(S);
-            return rc;
+            return fail(PK_ERR_OOM, "server host buffers could not be allocated");
         }
     }
     S->worker = std::thread(srv_loop, S);
@@ -1946,6 +2084,10 @@ int srv_submit(pk_server *S, const void *queries, int32_t nq, int32_t k, int32_t
     if (!S || !queries || nq < 1 || !ticket) return fail(PK_ERR_ARG, "bad arguments");
     if (nq > S->max_batch) return fail(PK_ERR_ARG, "request larger than the server's batch capacity");
     if (k < 1 || k > S->max_k || ef < k || ef > S->max_ef) return fail(PK_ERR_ARG, "k or ef outside the server's limits");
+    const size_t need = srv_layout(S->h, nq, k, ef).total;
+    if (need > S->arena_bytes)
+        return fail(PK_ERR_CAPACITY, "request needs " + std::to_string(need) + " bytes of device memory; the server holds " +
+                                         std::to_string(S->arena_bytes));
     auto r = std::make_shared<SrvRequest>();
     r->nq = nq;
     r->k = k;
@@ -2288,10 +2430,35 @@ int pk_index_search_fast_host_var(pk_index *h, const void *queries, int64_t nq, 
 int pk_server_create(pk_server **out, pk_index *h, int traversal, int slots, int32_t max_batch, int32_t max_k,
                      int32_t max_ef, int32_t expand) {
     try {
-        return srv_create(out, h, traversal, slots, max_batch, max_k, max_ef, expand);
+        return srv_create(out, h, traversal, slots, max_batch, max_k, max_ef, expand, 0);
     } catch (...) {
         return fail(PK_ERR_STATE, "pk_server_create: unexpected exception");
     }
+}
+
+int pk_server_create_with_memory(pk_server **out, pk_index *h, int traversal, int slots, int32_t max_batch,
+                                 int32_t max_k, int32_t max_ef, int32_t expand, int64_t device_bytes) {
+    try {
+        return srv_create(out, h, traversal, slots, max_batch, max_k, max_ef, expand, device_bytes);
+    } catch (...) {
+        return fail(PK_ERR_STATE, "pk_server_create_with_memory: unexpected exception");
+    }
+}
+
+int pk_server_memory(pk_server *s, int64_t *out) {
+    if (!s || !out) return fail(PK_ERR_ARG, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out[0] = (int64_t)s->arena_bytes;
+    out[1] = (int64_t)s->in_use;
+    out[2] = (int64_t)s->peak_in_use;
+    out[3] = s->deferred_for_memory;
+    return PK_OK;
+}
+
+int pk_server_request_bytes(pk_server *s, int32_t nq, int32_t k, int32_t ef, int64_t *bytes) {
+    if (!s || !bytes || nq < 1 || k < 1 || ef < 1) return fail(PK_ERR_ARG, "bad arguments");
+    *bytes = (int64_t)srv_layout(s->h, nq, k, std::min(ef, pk::kFastMaxEf)).total;
+    return PK_OK;
 }
 
 int pk_server_submit(pk_server *s, const void *queries, int32_t nq, int32_t k, int32_t ef, int64_t *ticket) {

@@ -47,6 +47,39 @@ def gmm_unit(n: int, nq: int, dim: int = 96, ncomp: int = 256, sigma: float = 0.
     return x[:n], x[n:]
 
 
+def embedding_like(n: int, nq: int, dim: int = 768, ncomp: int = 2048, zipf_s: float = 1.1, rank: int = 48,
+                   spread: float = 0.6, seed: int = 0, dtype=np.float16):
+    """Unit rows shaped like text embeddings: mixture components with
+    Zipf(zipf_s)-distributed sizes around random unit centres, each spread
+    over its own random rank-`rank` subspace with a decaying spectrum
+    (standard deviations proportional to 1/sqrt(i+1), total norm `spread`),
+    then normalised.  Embedding sets have a low intrinsic dimension; an
+    isotropic 768-dimensional spread instead makes every point nearly
+    equidistant from its cluster-mates, which no graph index searches well."""
+    rng = np.random.default_rng(seed)
+    centres = rng.standard_normal((ncomp, dim)).astype(np.float32)
+    centres /= np.linalg.norm(centres, axis=1, keepdims=True)
+    w = 1.0 / np.arange(1, ncomp + 1) ** zipf_s
+    lab = rng.choice(ncomp, size=n + nq, p=w / w.sum())
+    sv = 1.0 / np.sqrt(np.arange(1, rank + 1))
+    sv = (spread * sv / np.linalg.norm(sv)).astype(np.float32)
+    x = np.empty((n + nq, dim), dtype)
+    order = np.argsort(lab, kind="stable")
+    bounds = np.searchsorted(lab[order], np.arange(ncomp + 1))
+    for c in range(ncomp):
+        rows = order[bounds[c]:bounds[c + 1]]
+        if len(rows) == 0:
+            continue
+        basis, _ = np.linalg.qr(rng.standard_normal((dim, rank)).astype(np.float32))
+        for i in range(0, len(rows), 1 << 16):
+            r = rows[i:i + (1 << 16)]
+            z = rng.standard_normal((len(r), rank)).astype(np.float32) * sv
+            y = centres[c] + z @ basis.T
+            y /= np.linalg.norm(y, axis=1, keepdims=True)
+            x[r] = y.astype(dtype)
+    return x[:n], x[n:]
+
+
 def gmm_bytes(n: int, nq: int, dim: int = 128, ncomp: int = 64, sigma: float = 12.0, signed: bool = False,
               seed: int = 0):
     """uint8 or int8 rows: mixture centres uniform over the type's range,

@@ -11,7 +11,9 @@ recall@10 on the query pool (k = 10, one batch) is >= 0.95.  The stream is repla
 the GPU, batches of up to --max-batch queries).  Reported per rate: offered
 and served requests/s, p50/p99/max latency (submit to results on the host)
 and recall@10 of the served results against exact float64 ground truth.
-Data are seeded synthetic stand-ins for the configuration's shapes.
+Data are seeded synthetic stand-ins for the configuration's shapes; c5's
+768-dimensional rows come from datasets.embedding_like (Zipf-sized clusters,
+each spread over its own low-rank subspace, as text embeddings are).
 """
 from __future__ import annotations
 
@@ -48,8 +50,7 @@ def main(argv=None):
         _, pool = datasets.gmm_unit(0, a.pool, dim, ncomp=256, sigma=0.3, seed=a.seed)
     else:
         n, dim, metric, M, efc = a.n or 5_000_000, 768, "ip", a.M or 48, a.efc or 200
-        base, _ = datasets.gmm_unit(n, 0, dim, ncomp=2048, sigma=0.3, seed=a.seed, dtype=np.float16, zipf_s=1.1)
-        _, pool = datasets.gmm_unit(0, a.pool, dim, ncomp=2048, sigma=0.3, seed=a.seed, dtype=np.float16, zipf_s=1.1)
+        base, pool = datasets.embedding_like(n, a.pool, dim, ncomp=2048, zipf_s=1.1, seed=a.seed)
     idx = HNSWIndex(dim, base.dtype, metric, M=M, ef_construction=efc)
     idx.set_seed(a.seed)
     t0 = time.time()
@@ -61,8 +62,8 @@ def main(argv=None):
     shape, _ = idx.tune_fast(torch.from_numpy(pool[:a.max_batch]).cuda(), 50, 144)
     # recall@10 of the pool at k = 10 over an ef sweep: the stream at the target
     sweep = {}
-    ef95 = 512
-    for e in [64, 96, 128, 192, 256, 384, 512]:
+    ef95 = 1024
+    for e in [64, 96, 128, 192, 256, 384, 512, 768, 1024]:
         fi, _ = idx.search_fast(pool, 10, e)
         sweep[e] = round(datasets.recall_at_k(fi, gt, 10), 4)
         if sweep[e] >= 0.95:
@@ -70,7 +71,7 @@ def main(argv=None):
             break
     print(json.dumps({"config": a.config, "event": "ef_sweep", "k": 10, "recall_at_10": sweep, "ef95": ef95}),
           flush=True)
-    srv = Server(idx, a.traversal, slots=a.slots, max_batch=a.max_batch, max_k=100, max_ef=512)
+    srv = Server(idx, a.traversal, slots=a.slots, max_batch=a.max_batch, max_k=100, max_ef=max(512, ef95))
     rng = np.random.default_rng(a.seed + 1)
     for stream in a.streams.split(","):
         for rate in [float(x) for x in a.rates.split(",")]:

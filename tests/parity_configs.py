@@ -23,6 +23,13 @@ same queries on that file:
                where the two searches part; recall@k against exact float64
                ground truth must agree within 0.001.
 
+With --build the same configuration's graph is also built by the device
+(pk_index_build, batched insertion on the GPU) and both graphs are searched
+by the reference binary's AnnSearch at every ef: the two recall curves
+(against exact ground truth) show whether the device build reaches the
+reference build's quality at the same M and ef_construction (within two
+standard errors of a recall over nq x 10 labels).
+
 One JSON line per (k, ef); exit status 1 if any check fails.
 """
 from __future__ import annotations
@@ -62,6 +69,7 @@ def main(argv=None):
     p.add_argument("--efs", default="")
     p.add_argument("--ks", default="")
     p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--build", action="store_true", help="compare the device build with the reference build")
     p.add_argument("--max-fork-queries", type=int, default=100,
                    help="mismatched float queries replayed by the fork detector per (k, ef)")
     a = p.parse_args(argv)
@@ -89,6 +97,29 @@ def main(argv=None):
                 "metric": c["metric"], "M": c["M"], "ef_construction": c["efc"], "ref_build_s": round(build_s, 1),
                 "ref_build_threads": binfo.get("threads")}
         print(json.dumps(dict(head, event="built")), flush=True)
+        if a.build:
+            dpath = os.path.join(td, "dev.pkg")
+            t0 = time.time()
+            dev_idx = HNSWIndex(c["dim"], base.dtype, c["metric"], M=c["M"], ef_construction=c["efc"])
+            dev_idx.set_seed(a.seed)
+            dev_idx.build(base)
+            torch.cuda.synchronize()
+            dev_build_s = time.time() - t0
+            dev_idx.save(dpath)
+            dev_idx.close()
+            gt_b = gpu_knn(base, queries, 10, c["metric"], torch.device("cuda"))
+            for ef in efs:
+                rr, _, _ = oracle.ref_search(path, queries, 10, ef)
+                rd, _, _ = oracle.ref_search(dpath, queries, 10, ef)
+                r_ref = datasets.recall_at_k(rr, gt_b, 10)
+                r_dev = datasets.recall_at_k(rd, gt_b, 10)
+                tol = 2.0 * np.sqrt(max(r_ref * (1 - r_ref), 1e-4) / (10 * nq))
+                ok = r_dev >= r_ref - tol
+                ok_all &= bool(ok)
+                print(json.dumps(dict(head, event="build_recall", ef=ef, k=10, recall_reference_graph=round(r_ref, 5),
+                                      recall_device_graph=round(r_dev, 5), tolerance=round(float(tol), 5),
+                                      device_build_s=round(dev_build_s, 1), ok=bool(ok))), flush=True)
+            return 0 if ok_all else 1
         idx = HNSWIndex.load(path)
         g = oracle.OraGraph.load(path)
         dev = torch.device("cuda")
