@@ -1,6 +1,6 @@
 """Search parity at the benchmark configurations' full size (GPU + host).
 
-    python -m tests.parity_configs --config c2|c3u8|c3i8 [--nq N] [--efs 32,64] [--ks 10,100]
+    python -m tests.parity_configs --config c2|c3u8|c3i8|c5sub [--build] [--nq N] [--efs 32,64] [--ks 10,100]
 
 Test infrastructure, run by hand on a GPU machine (its output is summarised
 under profiles/): too long for the unit-test suite.  For each configuration
@@ -51,6 +51,9 @@ CONFIGS = {
     "c2": dict(n=1_000_000, nq=10_000, dim=96, metric="ip", M=32, efc=400, efs=[32, 64, 128, 256, 512], ks=[10, 100]),
     "c3u8": dict(n=1_000_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256], ks=[10]),
     "c3i8": dict(n=1_000_000, nq=10_000, dim=128, metric="l2", M=16, efc=200, efs=[16, 32, 64, 128, 256], ks=[10]),
+    # a 500k-row subset of the serving configuration (768-dimensional float16
+    # embedding-like rows, inner product, M = 48), for --build
+    "c5sub": dict(n=500_000, nq=2_000, dim=768, metric="ip", M=48, efc=200, efs=[64, 128, 256, 512], ks=[10]),
 }
 
 
@@ -58,6 +61,8 @@ def make(name, n, nq, seed):
     from pickle_b200 import datasets
     if name == "c2":
         return datasets.gmm_unit(n, nq, 96, ncomp=256, sigma=0.3, seed=seed)
+    if name == "c5sub":
+        return datasets.embedding_like(n, nq, 768, ncomp=2048, zipf_s=1.1, seed=seed)
     return datasets.gmm_bytes(n, nq, 128, ncomp=256, sigma=12.0, signed=name == "c3i8", seed=seed)
 
 
@@ -86,7 +91,7 @@ def main(argv=None):
     efs = [int(x) for x in a.efs.split(",")] if a.efs else c["efs"]
     ks = [int(x) for x in a.ks.split(",")] if a.ks else c["ks"]
     base, queries = make(a.config, n, nq, a.seed)
-    integer = base.dtype != np.float32
+    integer = base.dtype in (np.uint8, np.int8)
     ok_all = True
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "ref.pkg")

@@ -142,7 +142,7 @@ def test_fast_rejects_oversized_ef_and_shapes(gpu, ref_bin):
     idx.prepare_fast("f16")
     _, _, queries, _, _ = case_data("f32unit_ip")
     with pytest.raises(PickleError):
-        idx.search_fast(queries[:4], 10, 513)
+        idx.search_fast(queries[:4], 10, 1025)
     for bad in [(-1, 0, 0), (257, 0, 0), (0, 4, 0), (0, 16, 0), (0, 0, 9)]:
         with pytest.raises(PickleError):
             idx.set_fast_params(*bad)
