@@ -366,6 +366,8 @@ def run_ours(args):
         times, kernel_ms = [], []
         if path != "exact":
             idx.set_fast_timing(True)
+        # an NVTX range around the timed steps, for profilers to select
+        torch.cuda.nvtx.range_push(f"timed {path} {'mixed' if mixed else 'k10'}")
         with ClockSampler(local) as clk:
             for _ in range(args.steps):
                 flush.fill_(1)
@@ -377,6 +379,7 @@ def run_ours(args):
                 b.synchronize()
                 times.append(a.elapsed_time(b))
                 kernel_ms.append(idx.fast_timing()[0] if path != "exact" else times[-1])
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         if path != "exact":
             idx.set_fast_timing(False)

@@ -272,8 +272,8 @@ int pk_server_destroy(pk_server *s);
  * Limits: nq <= 65536 and ef <= 1024 (PK_ERR_ARG beyond them); a query that
  * outgrows the fixed scratch is not retried (PK_ERR_OVERFLOW; fall back to
  * pk_index_search_device).  The index's device must be current.  The first
- * call on a device looks up the array's address there: make it before any
- * stream capture.  All calls on a device share the array and keep its
+ * call on a device looks up the array's address there, and every call waits
+ * for its work on the stream before it returns.  All calls on a device share the array and keep its
  * contents between calls (the call clears what must start at zero); calls
  * that overlap on the GPU race on it, so serialise them.  Results equal
  * pk_index_search_device's. */

@@ -209,7 +209,10 @@ class HNSWIndex:
         return self.info()["num_layers"] if self._h is not None else 0
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the module's globals may be gone
+            pass
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -512,4 +515,7 @@ class Server:
             self._s = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the module's globals may be gone
+            pass

@@ -49,7 +49,6 @@ namespace {
 
 using namespace dev;
 
-constexpr uint32_t kExpanded = 0x80000000u;
 
 // ------------------------------------------------------- traversal distances
 // Traversal formats; both walk with tensor-core dot products (trav_dist_buf)
@@ -67,7 +66,7 @@ constexpr uint32_t kExpanded = 0x80000000u;
 struct TravView {
     const uint8_t *rows;      // traversal copy, row_bytes apart
     const uint8_t *zero_row;
-    int64_t row_bytes;
+    int32_t row_bytes;
     __device__ __forceinline__ const uint8_t *row(int32_t r) const {
         return r >= 0 ? rows + (int64_t)r * row_bytes : zero_row;
     }
@@ -109,7 +108,7 @@ __device__ __forceinline__ bool mbar_poll(uint64_t *bar, uint32_t parity) {
 
 struct RowFetch {
     uint8_t *buf;    // row t lands at buf + t * stride
-    int64_t stride;
+    int32_t stride;
     uint64_t *bar;
     uint32_t parity;
 };
@@ -195,7 +194,7 @@ __device__ __forceinline__ void mma_step(float (&c)[4], const uint32_t (&a)[4], 
 // row and no extra load.
 template <int TRAV>
 __device__ __forceinline__ void trav_dist_buf(bool ip, float qnorm,
-                                              float qfac, const RowFetch &f, int64_t data_bytes, const uint8_t *qbuf,
+                                              float qfac, const RowFetch &f, int32_t data_bytes, const uint8_t *qbuf,
                                               float *cd, int n, int lane) {
     auto xnorm = [&](int t) { return *reinterpret_cast<const float *>(f.buf + t * f.stride + data_bytes); };
     const int ks = (int)(data_bytes / 32);
@@ -320,66 +319,109 @@ struct SeenTable {
 
 // ------------------------------------------------------------ result list --
 // The ef best entries found so far, sorted by (distance, id), in registers:
-// lane l holds entries l*S .. l*S+S-1.  Empty slots hold (+inf, kEmpty); the
-// top bit of an id marks an entry already expanded.
+// lane l holds positions l*S .. l*S+S-1 of 32*S, and the list takes the last
+// ef of them, so that its ef-th entry - the bar a candidate must beat - is
+// always lane 31's last slot.  A distance is held as an unsigned key of the
+// same order (dist_key), so that (distance, id) compares as one 64-bit
+// integer.  The positions before the list hold key 0 (below every distance):
+// they count into each rank and never move.  Empty slots of the list hold
+// (kEmpty, kEmpty), above every entry.  Bit s of a lane's mask xm is set when
+// slot s cannot be expanded: its entry was expanded already, or the slot is
+// empty or before the list.  Keeping the marks in one word per lane (not in
+// the ids) makes finding the next entry to expand two bit operations and a
+// ballot, and leaves the ids as they are for the compares.
 
 constexpr uint32_t kEmpty = 0xffffffffu;
-
 __device__ __forceinline__ bool key_less(float da, uint32_t ia, float db, uint32_t ib) {
     return da < db || (da == db && ia < ib);
 }
 
+// A finite or infinite distance as an unsigned key in the same order, -0
+// taken as +0 (the two compare equal as floats): positive values gain the top
+// bit, negative ones are inverted.  Keys of distances lie in
+// [0x007fffff, 0xff800000]: 0 and kEmpty stay free for the list's bounds.
+__device__ __forceinline__ uint32_t dist_key(float d) {
+    uint32_t u = __float_as_uint(d);
+    u = u == 0x80000000u ? 0u : u;
+    return u ^ ((uint32_t)((int32_t)u >> 31) | 0x80000000u);
+}
+
+__device__ __forceinline__ uint64_t pack_key(uint32_t key, uint32_t id) { return ((uint64_t)key << 32) | id; }
+
 template <int S>
 struct RegList {
-    float d[S];
+    static constexpr uint32_t kSlots = S >= 32 ? 0xffffffffu : (1u << S) - 1u;
+    uint32_t k[S];
     uint32_t id[S];
+    uint32_t xm;
 
-    __device__ __forceinline__ void clear() {
+    // An empty list of the last L of the 32*S positions.
+    __device__ __forceinline__ void clear(int L, int lane) {
+        const int p0 = 32 * S - L;
 #pragma unroll
         for (int s = 0; s < S; s++) {
-            d[s] = __int_as_float(0x7f800000);
+            k[s] = lane * S + s < p0 ? 0u : kEmpty;
             id[s] = kEmpty;
+        }
+        xm = kSlots;
+    }
+
+    // The first position of an empty list of L: the entry point (not yet
+    // expanded).
+    __device__ __forceinline__ void put_first(int L, uint32_t nk, uint32_t nid, int lane) {
+        const int p0 = 32 * S - L;
+        if (lane == p0 / S) {
+#pragma unroll
+            for (int s = 0; s < S; s++)
+                if (s == p0 % S) {
+                    k[s] = nk;
+                    id[s] = nid;
+                }
+            xm &= ~(1u << (p0 % S));
         }
     }
 
-    // Inserts (nd, nid) (nid without the flag; nd finite) at its rank unless
-    // the list holds nid already; the last entry of the 32*S falls off.
-    __device__ __forceinline__ void insert(float nd, uint32_t nid, int lane) {
+    // Inserts (nk, nid) at its rank, unexpanded, unless the list holds nid
+    // already; the last entry of the 32*S falls off.
+    __device__ __forceinline__ void insert(uint32_t nk, uint32_t nid, int lane) {
+        const uint64_t x = pack_key(nk, nid);
         int c = 0;
         bool dup = false;
 #pragma unroll
         for (int s = 0; s < S; s++) {
-            const uint32_t m = id[s] & ~kExpanded;
-            c += key_less(d[s], m, nd, nid) ? 1 : 0;
-            dup |= m == nid;
+            c += pack_key(k[s], id[s]) < x ? 1 : 0;
+            dup |= id[s] == nid;
         }
         if (__any_sync(kFull, dup)) return;
         // sorted: lanes before the rank have c == S, lanes after it c == 0
-        const float pd = __shfl_up_sync(kFull, d[S - 1], 1);
+        const uint32_t pk = __shfl_up_sync(kFull, k[S - 1], 1);
         const uint32_t pi = __shfl_up_sync(kFull, id[S - 1], 1);
         const int pc = __shfl_up_sync(kFull, c, 1);
+        const uint32_t pb = __shfl_up_sync(kFull, xm >> (S - 1), 1) & 1u;
         const bool here = c > 0 || lane == 0 || pc == S;  // the new entry lands in slot c of this lane
         if (c < S) {
 #pragma unroll
             for (int s = S - 1; s >= 0; s--) {
                 if (s > 0 && s > c) {
-                    d[s] = d[s - 1];
+                    k[s] = k[s - 1];
                     id[s] = id[s - 1];
                 } else if (s == c) {
-                    d[s] = here ? nd : pd;
+                    k[s] = here ? nk : pk;
                     id[s] = here ? nid : pi;
                 }
             }
+            // the marks move with their entries: slots below c stay, slots
+            // above shift up one, slot c takes the new entry's (clear) or the
+            // previous lane's last mark
+            const uint32_t low = (1u << c) - 1u;
+            xm = ((xm & low) | ((xm << 1) & ~(low | (1u << c))) | ((here ? 0u : pb) << c)) & kSlots;
         }
     }
 
-    // Marks the first unexpanded entry among the slots in vmask as expanded
-    // and returns its id, or -1 if there is none.
-    __device__ __forceinline__ int32_t take_first(unsigned vmask, int lane) {
-        unsigned un = 0;
-#pragma unroll
-        for (int s = 0; s < S; s++) un |= ((id[s] & kExpanded) == 0 ? 1u : 0u) << s;
-        un &= vmask;
+    // Marks the first expandable entry as expanded and returns its id, or -1
+    // if there is none.
+    __device__ __forceinline__ int32_t take_first(int lane) {
+        const unsigned un = ~xm & kSlots;
         const unsigned b = __ballot_sync(kFull, un != 0);
         if (b == 0) return -1;
         const int fl = __ffs(b) - 1;
@@ -388,28 +430,15 @@ struct RegList {
             const int fs = __ffs(un) - 1;
 #pragma unroll
             for (int s = 0; s < S; s++)
-                if (s == fs) {
-                    v = (int32_t)id[s];
-                    id[s] |= kExpanded;
-                }
+                if (s == fs) v = (int32_t)id[s];
+            xm |= 1u << fs;
         }
         return __shfl_sync(kFull, v, fl);
     }
 
-    // The entry in slot ws of lane wl (distance, id without the flag).
-    __device__ __forceinline__ void at(int wl, int ws, float &wd, uint32_t &wi, int lane) const {
-        float x = 0.f;
-        uint32_t y = 0;
-        if (lane == wl) {
-#pragma unroll
-            for (int s = 0; s < S; s++)
-                if (s == ws) {
-                    x = d[s];
-                    y = id[s] & ~kExpanded;
-                }
-        }
-        wd = __shfl_sync(kFull, x, wl);
-        wi = __shfl_sync(kFull, y, wl);
+    // The list's last entry (its ef-th) as a packed key.
+    __device__ __forceinline__ uint64_t last() const {
+        return pack_key(__shfl_sync(kFull, k[S - 1], 31), __shfl_sync(kFull, id[S - 1], 31));
     }
 };
 
@@ -439,15 +468,13 @@ __device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, i
 
 // ------------------------------------------------------------------ walk ---
 // Blocks of 256 threads resident per SM that each instantiation is compiled
-// for: three (80 registers per thread, 24 warps per SM) wherever the list and
-// the rest fit 80 registers without spills (ptxas -v): every width up to 4
-// slots, FP16 with one parent per step up to 16 slots (ef <= 512), and
-// otherwise up to 8 slots except FP8 with four parents; two (up to 128
-// registers, 16 warps) for the rest.
+// for: three (80 registers per thread, 24 warps per SM) up to 8 slots per lane
+// (ef <= 256) except FP8 with four parents, where the list and the rest fit 80
+// registers without spills (ptxas -v); two (up to 128 registers, 16 warps) for
+// wider lists.  At 12 and 16 slots the 80-register build spills, and the
+// 16-warp one measured 11-15% faster on 2M x 128 FP16 rows (ef = 384, 512).
 constexpr int walk_min_blocks(int trav, int s, int exp) {
-    return s <= 4 ? 3
-           : (trav == kTravF16 ? (exp == 1 ? s <= 16 : s <= 8) : (exp == 1 && s <= 8)) ? 3
-                                                                                        : 2;
+    return s <= 4 ? 3 : (s <= 8 && (trav == kTravF16 || exp == 1)) ? 3 : 2;
 }
 
 // EXP bounds the parents expanded per step: the walk with one parent per
@@ -475,16 +502,17 @@ __global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
     if (lane == 0) mbar_init(bar);
     __syncwarp();
     uint8_t *qbuf = my + lay.qbuf;
-    RowFetch f{my + lay.rowbuf, lay.stride, bar, 0u};
+    RowFetch f{my + lay.rowbuf, (int32_t)lay.stride, bar, 0u};
 
-    const TravView tv{a.trav, a.trav_zero, a.trav_row_bytes};
+    const TravView tv{a.trav, a.trav_zero, (int32_t)a.trav_row_bytes};
     const bool ip = gp->metric == PK_METRIC_IP;
-    const int64_t tdb = a.trav_data_bytes;
+    const int32_t tdb = (int32_t)a.trav_data_bytes;
     const int enter_level = gp->enter_level;
     const int rb = a.rb;
     const int expand = max(1, min(a.expand, EXP));
     const DevLayer L0 = gp->L[0];
-    const int64_t lim0 = min(L0.lcap, a.trav_rows);
+    const int32_t lim0 = (int32_t)min(L0.lcap, a.trav_rows);
+    const int32_t cap0 = (int32_t)L0.cap;
     const float kInf = __int_as_float(0x7f800000);
 
     const int64_t nlim = a.qcount ? (int64_t)*a.qcount : a.nq;
@@ -563,14 +591,18 @@ __global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
             enter = dn >= 0 ? dn : gp->L[level - 1].ent;
         }
 
+        // the upper layers' counters go out now: fewer registers live below
+        if (a.counters && lane == 0) {
+            int32_t *cp = a.counters + q * 6;
+            cp[0] = cnt[0];
+            cp[1] = cnt[1];
+            cp[2] = cnt[2];
+        }
+
         // ---- layer 0: best-first walk over the register list ----
         RegList<S> list;
-        list.clear();
-        const int wl = (L - 1) / S, wsl = (L - 1) % S;
-        const int own = L - lane * S;  // slots of this lane below L
-        const unsigned vmask = own <= 0 ? 0u : own >= S ? (S >= 32 ? ~0u : (1u << S) - 1u) : (1u << own) - 1u;
-        float wd = kInf;
-        uint32_t wi = kEmpty & ~kExpanded;
+        list.clear(L, lane);
+        uint64_t wk = pack_key(kEmpty, kEmpty);
         if (!failed) {
             seen.clear(lane);
             __syncwarp();
@@ -581,13 +613,10 @@ __global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
         if (!failed) {
             trav_dist_buf<TRAV>(ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
             const float d0 = cd[0];
-            if (lane == 0) {
-                list.d[0] = d0;
-                list.id[0] = (uint32_t)enter;
-                seen.test_and_mark(enter);
-            }
+            list.put_first(L, dist_key(d0), (uint32_t)enter, lane);
+            if (lane == 0) seen.test_and_mark(enter);
             __syncwarp();
-            list.at(wl, wsl, wd, wi, lane);
+            wk = list.last();
         }
         auto flush0 = [&](int nn) -> bool {
             if (!fetch_rows(f, tv, crow, nn, lane)) return false;
@@ -595,32 +624,34 @@ __global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
             cnt[4] += nn;
             for (int i0 = 0; i0 < nn; i0 += 32) {
                 const int i = i0 + lane;
-                float nd = kInf;
-                uint32_t nid = kEmpty;
+                uint32_t nk = kEmpty, nid = kEmpty;
+                bool ok = false;
                 if (i < nn) {
-                    nd = cd[i];
+                    const float nd = cd[i];
+                    nk = dist_key(nd);
                     nid = (uint32_t)crow[i];
+                    ok = nd < kInf;
                 }
-                unsigned m = __ballot_sync(kFull, i < nn && nd < kInf && key_less(nd, nid, wd, wi));
+                unsigned m = __ballot_sync(kFull, ok && pack_key(nk, nid) < wk);
                 while (m) {
                     const int src = __ffs(m) - 1;
                     m &= m - 1;
-                    const float xd = __shfl_sync(kFull, nd, src);
+                    const uint32_t xk = __shfl_sync(kFull, nk, src);
                     const uint32_t xi = __shfl_sync(kFull, nid, src);
-                    if (!key_less(xd, xi, wd, wi)) continue;
-                    list.insert(xd, xi, lane);
-                    list.at(wl, wsl, wd, wi, lane);
+                    if (!(pack_key(xk, xi) < wk)) continue;
+                    list.insert(xk, xi, lane);
+                    wk = list.last();
                 }
             }
             __syncwarp();
             return true;
         };
-        int64_t iters = 0;
+        int32_t iters = 0;
         while (!failed) {
             int32_t pc[4];
 #pragma unroll
-            for (int p = 0; p < 4; p++) pc[p] = p < EXP && p < expand ? list.take_first(vmask, lane) : -1;
-            if (pc[0] < 0 || ++iters > L0.lcap) break;
+            for (int p = 0; p < 4; p++) pc[p] = p < EXP && p < expand ? list.take_first(lane) : -1;
+            if (pc[0] < 0 || ++iters > lim0) break;
             // degrees and the first 64 slots of each parent's list, all in flight
             int pdeg[4];
             int32_t pa0[4], pa1[4];
@@ -630,10 +661,10 @@ __global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
                 pa0[p] = -1;
                 pa1[p] = -1;
                 if (pc[p] >= 0) {
-                    const int64_t base = (int64_t)pc[p] * L0.cap;
+                    const int64_t base = (int64_t)pc[p] * cap0;
                     pdeg[p] = L0.deg[pc[p]];
-                    if (lane < L0.cap) pa0[p] = L0.adj[base + lane];
-                    if (32 + lane < L0.cap) pa1[p] = L0.adj[base + 32 + lane];
+                    if (lane < cap0) pa0[p] = L0.adj[base + lane];
+                    if (32 + lane < cap0) pa1[p] = L0.adj[base + 32 + lane];
                 }
             }
             int n = 0;
@@ -641,13 +672,13 @@ __global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
             for (int p = 0; p < EXP; p++) {
                 if (pc[p] < 0 || failed) continue;
                 const int deg = pdeg[p];
-                const int64_t base = (int64_t)pc[p] * L0.cap;
+                const int64_t base = (int64_t)pc[p] * cap0;
                 cnt[3]++;
                 cnt[5] += deg;
                 for (int j0 = 0; j0 < deg; j0 += 32) {
                     const int j = j0 + lane;
                     int32_t v = -1;
-                    if (j < deg) v = (j < L0.cap && j0 == 0) ? pa0[p] : (j < L0.cap && j0 == 32) ? pa1[p] : L0.adj[base + j];
+                    if (j < deg) v = (j < cap0 && j0 == 0) ? pa0[p] : (j < cap0 && j0 == 32) ? pa1[p] : L0.adj[base + j];
                     const bool fresh = v >= 0 && v < lim0 && seen.test_and_mark(v);
                     if (!append_pending(fresh, v, v, crow, cid, n, rb, lane, flush0)) {
                         failed = true;
@@ -665,13 +696,14 @@ __global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
         int32_t *out = a.cand + q * a.cand_stride;
 #pragma unroll
         for (int s = 0; s < S; s++) {
-            const int i = lane * S + s;
-            if (i < L) out[i] = list.d[s] < kInf ? (int32_t)(list.id[s] & ~kExpanded) : -1;
+            const int i = lane * S + s - (32 * S - L);
+            if (i >= 0) out[i] = list.id[s] == kEmpty ? -1 : (int32_t)list.id[s];
         }
         if (a.counters && lane == 0) {
             int32_t *cp = a.counters + q * 6;
-#pragma unroll
-            for (int i = 0; i < 6; i++) cp[i] = cnt[i];
+            cp[3] = cnt[3];
+            cp[4] = cnt[4];
+            cp[5] = cnt[5];
         }
         __syncwarp();
     }

@@ -124,7 +124,24 @@ struct FastCtx {
     // optional timing of the last launch: before the walk, after it, after
     // the re-rank (created on first use)
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    // per-query ef: one stream per list width, so that the widths' launches
+    // run side by side and one width's tail does not hold the next back
+    // (forked from and joined to the caller's stream with events; created on
+    // first use)
+    cudaStream_t aux[pk::kSlotClasses] = {};
+    cudaEvent_t fork = nullptr, join[pk::kSlotClasses] = {};
 };
+
+// Releases a context's streams and events (not its buffers).
+void release_ctx_sync(FastCtx &c) {
+    for (cudaEvent_t &e : c.ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t &e : c.join)
+        if (e) cudaEventDestroy(e);
+    if (c.fork) cudaEventDestroy(c.fork);
+    for (cudaStream_t &t : c.aux)
+        if (t) cudaStreamDestroy(t);
+}
 
 }  // namespace
 
@@ -910,9 +927,20 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
             if (!e) PK_CUDA(cudaEventCreate(&e));
         PK_CUDA(cudaEventRecord(c.ev[0], s));
     }
+    if (binned) {
+        if (!c.fork) PK_CUDA(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
+        PK_CUDA(cudaEventRecord(c.fork, s));
+    }
     for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
         const int sl = pk::slot_class_width(cls);
         if (!binned && sl != slots) continue;
+        cudaStream_t ls = s;
+        if (binned) {
+            if (!c.aux[cls]) PK_CUDA(cudaStreamCreateWithFlags(&c.aux[cls], cudaStreamNonBlocking));
+            if (!c.join[cls]) PK_CUDA(cudaEventCreateWithFlags(&c.join[cls], cudaEventDisableTiming));
+            ls = c.aux[cls];
+            PK_CUDA(cudaStreamWaitEvent(ls, c.fork, 0));
+        }
         PK_TRY(walk_shape(h, ws, cls));
         a.rb = ws.rb;
         a.hlog2 = ws.hlog2;
@@ -924,7 +952,11 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
         a.work = c.d_work + kWorkCounters + cls;
         a.qlist = binned ? c.d_lists + cls * nq : nullptr;
         a.qcount = binned ? c.d_work + kWorkCounts + cls : nullptr;
-        PK_CUDA(pk::launch_walk(h->dg, h->trav, sl, a, (int)grid, ws.wpb, ws.smem, s));
+        PK_CUDA(pk::launch_walk(h->dg, h->trav, sl, a, (int)grid, ws.wpb, ws.smem, ls));
+        if (binned) {
+            PK_CUDA(cudaEventRecord(c.join[cls], ls));
+            PK_CUDA(cudaStreamWaitEvent(s, c.join[cls], 0));
+        }
     }
     if (timed) PK_CUDA(cudaEventRecord(c.ev[1], s));
 
@@ -1008,8 +1040,7 @@ int init_handle(pk_index *h, int metric, int dtype, int64_t dim, int64_t M, int6
 }
 
 void free_fast_ctx(pk_index *h, FastCtx &c) {
-    for (cudaEvent_t &e : c.ev)
-        if (e) cudaEventDestroy(e);
+    release_ctx_sync(c);
     dfree(h, c.d_work, 4 * (size_t)c.work_n);
     dfree(h, c.d_cand, 4 * (size_t)c.cand_n);
     dfree(h, c.d_lists, 4 * (size_t)c.lists_n);
@@ -2005,9 +2036,9 @@ void srv_loop(pk_server *S) {
 void srv_free(pk_server *S) {
     for (SrvSlot &sl : S->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
-        // the slot's scratch lives in the arena: only its events are its own
-        for (cudaEvent_t &e : sl.ctx.ev)
-            if (e) cudaEventDestroy(e);
+        // the slot's scratch lives in the arena: only its streams and events
+        // are its own
+        release_ctx_sync(sl.ctx);
         cudaFreeHost(sl.h_q);
         cudaFreeHost(sl.h_k);
         cudaFreeHost(sl.h_ef);

@@ -19,9 +19,8 @@
 //    outgrows the fixed scratch is not retried: the call returns
 //    PK_ERR_OVERFLOW and the caller can fall back to pk_index_search_device.
 //  * The first call on a device looks up the array's device address there
-//    (with that device current); make that first call before any stream
-//    capture begins.  Every call waits for its own work on the stream before
-//    it returns (it reads the overflow count back).
+//    (with that device current).  Every call waits for its own work on the
+//    stream before it returns (it reads the overflow count back).
 //  * Every call on a device shares the one array, which keeps the previous
 //    call's contents.  What must start from zero is cleared by the call: the
 //    work counters on every call, and the visited bitmaps, which sit at the
