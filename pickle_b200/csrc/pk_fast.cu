@@ -385,37 +385,49 @@ struct RegList {
     // already; the last entry of the 32*S falls off.
     __device__ __forceinline__ void insert(uint32_t nk, uint32_t nid, int lane) {
         const uint64_t x = pack_key(nk, nid);
-        int c = 0;
-        bool dup = false;
+        // one bit per slot below the new entry (a prefix: the slots are
+        // sorted) and per slot holding its id, folded by OR trees so that
+        // the rank is a popcount, not a chain of S dependent adds
+        uint32_t lt[S], eq[S];
 #pragma unroll
         for (int s = 0; s < S; s++) {
-            c += pack_key(k[s], id[s]) < x ? 1 : 0;
-            dup |= id[s] == nid;
+            lt[s] = pack_key(k[s], id[s]) < x ? (1u << s) : 0u;
+            eq[s] = id[s] == nid ? 1u : 0u;
         }
-        if (__any_sync(kFull, dup)) return;
+#pragma unroll
+        for (int w = 1; w < S; w <<= 1)
+#pragma unroll
+            for (int s = 0; s + w < S; s += 2 * w) {
+                lt[s] |= lt[s + w];
+                eq[s] |= eq[s + w];
+            }
+        if (__any_sync(kFull, eq[0] != 0u)) return;
+        const int c = __popc(lt[0]);
         // sorted: lanes before the rank have c == S, lanes after it c == 0
         const uint32_t pk = __shfl_up_sync(kFull, k[S - 1], 1);
         const uint32_t pi = __shfl_up_sync(kFull, id[S - 1], 1);
         const int pc = __shfl_up_sync(kFull, c, 1);
         const uint32_t pb = __shfl_up_sync(kFull, xm >> (S - 1), 1) & 1u;
         const bool here = c > 0 || lane == 0 || pc == S;  // the new entry lands in slot c of this lane
-        if (c < S) {
+        const uint32_t ck = here ? nk : pk, ci = here ? nid : pi;
+        // slots above c shift up one, slot c takes the entry; a lane with
+        // c == S keeps all its slots
 #pragma unroll
-            for (int s = S - 1; s >= 0; s--) {
-                if (s > 0 && s > c) {
-                    k[s] = k[s - 1];
-                    id[s] = id[s - 1];
-                } else if (s == c) {
-                    k[s] = here ? nk : pk;
-                    id[s] = here ? nid : pi;
-                }
+        for (int s = S - 1; s >= 0; s--) {
+            if (s > 0 && s > c) {
+                k[s] = k[s - 1];
+                id[s] = id[s - 1];
+            } else if (s == c) {
+                k[s] = ck;
+                id[s] = ci;
             }
-            // the marks move with their entries: slots below c stay, slots
-            // above shift up one, slot c takes the new entry's (clear) or the
-            // previous lane's last mark
-            const uint32_t low = (1u << c) - 1u;
-            xm = ((xm & low) | ((xm << 1) & ~(low | (1u << c))) | ((here ? 0u : pb) << c)) & kSlots;
         }
+        // the marks move with their entries: slots below c stay, slots above
+        // shift up one, slot c takes the new entry's (clear) or the previous
+        // lane's last mark
+        const uint32_t bitc = c < 32 ? 1u << c : 0u;
+        const uint32_t low = bitc - 1u;
+        xm = ((xm & low) | ((xm << 1) & ~(low | bitc)) | (here || pb == 0u ? 0u : bitc)) & kSlots;
     }
 
     // Marks the first expandable entry as expanded and returns its id, or -1
@@ -467,21 +479,21 @@ __device__ __forceinline__ void warp_argmin(const float *cd, int n, float &bd, i
 }
 
 // ------------------------------------------------------------------ walk ---
-// Blocks of 256 threads resident per SM that each instantiation is compiled
-// for: three (80 registers per thread, 24 warps per SM) up to 8 slots per lane
-// (ef <= 256) except FP8 with four parents, where the list and the rest fit 80
-// registers without spills (ptxas -v); two (up to 128 registers, 16 warps) for
-// wider lists.  At 12 and 16 slots the 80-register build spills, and the
-// 16-warp one measured 11-15% faster on 2M x 128 FP16 rows (ef = 384, 512).
-constexpr int walk_min_blocks(int trav, int s, int exp) {
-    return s <= 4 ? 3 : (s <= 8 && (trav == kTravF16 || exp == 1)) ? 3 : 2;
+// Registers per thread that each instantiation is compiled for: 80 (24 warps
+// per SM) up to 8 slots per lane (ef <= 256) except FP8 with four parents,
+// where the list and the rest fit without spills (ptxas -v); 128 (16 warps)
+// for wider lists.  At 12 and 16 slots the 80-register build spills, and 128
+// registers measured 11-15% faster than 80 on 2M x 128 FP16 rows (ef = 384,
+// 512) and 2-10% faster than 88 or 96 (which fit without spills, 20-22 warps).
+constexpr int walk_max_regs(int trav, int s, int exp) {
+    return s <= 4 ? 80 : (s <= 8 && (trav == kTravF16 || exp == 1)) ? 80 : 128;
 }
 
 // EXP bounds the parents expanded per step: the walk with one parent per
 // step (the default) has its own instantiation, a quarter of the layer-0
 // loop's code of the one that takes up to four.
 template <int TRAV, int S, int EXP>
-__global__ void __launch_bounds__(256, walk_min_blocks(TRAV, S, EXP))
+__global__ void __maxnreg__(walk_max_regs(TRAV, S, EXP))
     walk_kernel(const DevGraph *__restrict__ gp, const WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;

@@ -138,3 +138,21 @@ def compare_float_results(ids_a, d_a, ids_b, d_b, rel=1e-6):
                 break
         ok += same
     return ok / len(ids_a)
+
+
+def build_recall_tolerance(ref_recalls, dev_recalls, labels):
+    """Two standard errors of (mean device-graph recall - mean reference-graph
+    recall), each side's mean taken over graphs built from different seeds:
+    the graphs' spread around their mean (sample variance over seeds, when
+    there are several) plus the sampling error of one recall over `labels`
+    binary outcomes (queries x k)."""
+    r = np.asarray(ref_recalls, np.float64)
+    d = np.asarray(dev_recalls, np.float64)
+    m = float(r.mean())
+    samp = max(m * (1.0 - m), 1e-4) / labels
+    var = samp / len(r) + samp / len(d)
+    if len(r) > 1:
+        var += r.var(ddof=1) / len(r)
+    if len(d) > 1:
+        var += d.var(ddof=1) / len(d)
+    return 2.0 * float(np.sqrt(var))

@@ -12,7 +12,7 @@ import pytest
 
 import oracle
 from pickle_b200 import HNSWIndex, datasets
-from tests.helpers import case_data, levels_for
+from tests.helpers import build_recall_tolerance, case_data, levels_for
 
 pytestmark = pytest.mark.gpu
 
@@ -85,17 +85,29 @@ def test_saved_build_reloads_identically(gpu, tmp_path):
 
 @pytest.mark.parametrize("name", ["f32int_l2", "f32unit_ip"])
 def test_batched_build_reaches_reference_recall(name, gpu, ref_bin, tmp_path):
+    """Three batched device builds (seeds 3-5) against three builds by the
+    reference's parallel Build (level draws from seeds 0-2): the device graphs'
+    mean recall@10 is at least the reference graphs' mean minus two standard
+    errors of the difference (the graphs' spread over seeds and the sampling
+    error of a recall over 200 queries x 10)."""
     metric, base, queries, M, efc = case_data(name)
     n = len(base)
     gt, _ = datasets.exact_knn(base, queries, 10, metric)
-    rpath = str(tmp_path / "ref.pkg")
-    oracle.ref_build(base, metric, M, efc, rpath, threads=8)
-    idx = HNSWIndex(base.shape[1], base.dtype, metric, M, efc)
-    idx.set_seed(3)
-    idx.build(base)
-    for ef in (16, 32, 64):
-        ri, _, _ = oracle.ref_search(rpath, queries, 10, ef, threads=4)
-        ids, _ = idx.search(queries, 10, ef)
-        r_ref = datasets.recall_at_k(ri, gt, 10)
-        r_dev = datasets.recall_at_k(ids, gt, 10)
-        assert r_dev >= r_ref - 0.02, (ef, r_dev, r_ref)
+    efs = (16, 32, 64)
+    r_ref = {ef: [] for ef in efs}
+    r_dev = {ef: [] for ef in efs}
+    for s in range(3):
+        rpath = str(tmp_path / f"ref{s}.pkg")
+        oracle.ref_build(base, metric, M, efc, rpath, threads=8, levels=levels_for(n, M, s))
+        idx = HNSWIndex(base.shape[1], base.dtype, metric, M, efc)
+        idx.set_seed(3 + s)
+        idx.build(base)
+        for ef in efs:
+            ri, _, _ = oracle.ref_search(rpath, queries, 10, ef, threads=4)
+            ids, _ = idx.search(queries, 10, ef)
+            r_ref[ef].append(datasets.recall_at_k(ri, gt, 10))
+            r_dev[ef].append(datasets.recall_at_k(ids, gt, 10))
+        idx.close()
+    for ef in efs:
+        tol = build_recall_tolerance(r_ref[ef], r_dev[ef], 10 * len(queries))
+        assert np.mean(r_dev[ef]) >= np.mean(r_ref[ef]) - tol, (ef, r_dev[ef], r_ref[ef], tol)
