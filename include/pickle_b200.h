@@ -171,6 +171,30 @@ int pk_index_search_fast_host_var(pk_index *h, const void *queries, int64_t nq, 
  * pk_index_tune_fast_classes.  No counterpart in the reference. */
 int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter_log2, int32_t warps_per_block);
 
+/* Second level of the walk's visited filter: besides its table of recently
+ * seen ids in shared memory, each walk warp keeps a larger table of the ids it
+ * met in global memory (8-way sets of exact 16-bit tags, cleared per query,
+ * a few to a few tens of KB per warp so that the resident warps' tables stay
+ * in L2), which spares the walk most of the rows it would otherwise fetch and
+ * score again after the shared-memory table forgot them.  log2_sets = 0 sizes
+ * each width's tables by its list width (the default), -1 turns them off,
+ * 1..20 gives every width 2^log2_sets sets of 16 bytes.  The tables are
+ * allocated with the search's other buffers (their size grows with the warps
+ * of a launch, not with the batch); when that allocation fails the walk runs
+ * without them.  The results do not depend on this setting.  No counterpart
+ * in the reference. */
+int pk_index_set_fast_visited(pk_index *h, int32_t log2_sets);
+
+/* Insertion into the walk's result list: a list of 6 or more slots of 32
+ * entries per lane (ef > 160) takes the winners of a 32-candidate chunk (the
+ * candidates that beat its last entry) one at a time, or, when at least
+ * min_winners of them win, all at once by a merge (sorted across the warp,
+ * ranked in the list by binary search, moved through shared memory).  Either
+ * way the list afterwards is the same.  0 = a threshold by list width (the
+ * default), -1 = never merge, 1..32 = merge from that many winners.  No
+ * counterpart in the reference. */
+int pk_index_set_fast_merge(pk_index *h, int32_t min_winners);
+
 /* Measurement: with timing enabled, each pk_index_search_fast /
  * pk_index_search_fast_host call on the handle records CUDA events on its
  * stream around the walk kernel and the re-rank kernel;

@@ -71,6 +71,8 @@ def lib() -> ctypes.CDLL:
         L.pk_index_search_fast_host.argtypes = [P, VP, I64, I32, I32, VP, VP, I32]
         L.pk_index_set_fast_params.argtypes = [P, I32, I32, I32]
         L.pk_index_set_fast_timing.argtypes = [P, ctypes.c_int]
+        L.pk_index_set_fast_visited.argtypes = [P, I32]
+        L.pk_index_set_fast_merge.argtypes = [P, I32]
         L.pk_index_fast_timing.argtypes = [P, VP, VP]
         L.pk_index_tune_fast.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
         L.pk_index_tune_fast_classes.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
@@ -313,6 +315,16 @@ class HNSWIndex:
         """Launch shape of the fast walk (0 = default): rows fetched per round trip, log2 of the
         recently-seen-id table's slots, warps per block.  Results do not depend on the shape."""
         _check(lib().pk_index_set_fast_params(self._h, rows_per_batch, filter_log2, warps_per_block))
+
+    def set_fast_visited(self, log2_sets: int = 0) -> None:
+        """The walk's second-level visited tables in L2: 0 = sized by list width (default),
+        -1 = off, 1..20 = 2^log2_sets sets of eight tags per warp.  Results do not depend on it."""
+        _check(lib().pk_index_set_fast_visited(self._h, int(log2_sets)))
+
+    def set_fast_merge(self, min_winners: int = 0) -> None:
+        """Wide lists merge a chunk's winners at once from min_winners of them (0 = by list width,
+        -1 = never: one at a time).  Results do not depend on it."""
+        _check(lib().pk_index_set_fast_merge(self._h, int(min_winners)))
 
     def set_fast_timing(self, enable: bool) -> None:
         """Record CUDA events around the walk and re-rank kernels of each fast search."""

@@ -20,17 +20,20 @@
 //     registers (lane l owns entries l*S .. l*S+S-1); each iteration expands
 //     the `expand` best unexpanded entries, filters their neighbours through
 //     a table of recently seen ids in shared memory (exact 16-bit tags in
-//     4-way sets where the ids allow, least recently inserted out),
+//     4-way sets where the ids allow, least recently inserted out) and then,
+//     for what that table does not hold, through a larger per-warp table in
+//     global memory that stays in L2 (exact 16-bit tags in 8-way sets),
 //     fetches the new rows with one bulk copy (cp.async.bulk) per row onto a
 //     per-warp mbarrier, and inserts what beats the worst listed entry;
 //   * the walk ends when the first ef entries are all expanded, and their
 //     ids are written out.
-//   The visited table forgets ids on collisions, which costs a recomputed
+//   The visited tables forget ids on collisions, which costs a recomputed
 //   distance but never a duplicate: an insertion of an id the list holds is
 //   dropped, and a node that left the list (or was turned away) cannot come
 //   back, since the worst listed distance never rises.  So the list after
 //   each step - the best ef of what was listed and what was met - does not
-//   depend on the table's size or on the batch order.
+//   depend on the tables' sizes (or on whether the L2 table is used at all)
+//   or on the batch order.
 //
 // rerank_kernel (one query per warp): exact distances from the original
 // vectors for the ef listed ids, sorted by (distance, id); the k best are
@@ -317,6 +320,83 @@ struct SeenTable {
     }
 };
 
+// ------------------------------------------------------ visited ids in L2 --
+// Second level of the visited filter, for ids the shared-memory table does
+// not hold: a per-warp table in global memory of 2^log2sets sets of eight
+// 16-bit tags (16 bytes, one load), cleared at the start of each query and
+// sized by the list width to hold the ids a walk of that width meets (a few
+// to a few tens of KB per warp: the resident warps' tables stay in L2).  Tags
+// are exact as in the shared-memory table: the scrambled id's top bits pick
+// the set and its remaining tbits (<= 15), plus one, are the tag, so a hit is
+// always a real revisit; a full set forgets its oldest id.  Lanes of a warp
+// that update one set at once may lose one of the two ids (a recomputed
+// distance later, never a wrong answer).
+struct L2Seen {
+    uint4 *sets;      // this warp's table, or null
+    int nsets;
+    uint32_t bmask;
+    int tbits;
+
+    // the set index of v, and its tag
+    __device__ __forceinline__ uint32_t set_of(int32_t v, uint32_t &tag) const {
+        const uint32_t h = ((uint32_t)v * 2654435761u) & bmask;
+        tag = (h & ((1u << tbits) - 1u)) + 1u;
+        return h >> tbits;
+    }
+};
+
+__device__ __forceinline__ uint4 ld_cg4(const uint4 *p) {
+    uint4 r;
+    asm volatile("ld.global.cg.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "l"(p)
+                 : "memory");
+    return r;
+}
+__device__ __forceinline__ void st_cg4(uint4 *p, uint4 v) {
+    asm volatile("st.global.cg.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+                 : "memory");
+}
+__device__ __forceinline__ bool set_has(uint4 x, uint32_t tag) {
+    const uint32_t t2 = tag * 0x10001u;
+    return (__vcmpeq2(x.x, t2) | __vcmpeq2(x.y, t2) | __vcmpeq2(x.z, t2) | __vcmpeq2(x.w, t2)) != 0u;
+}
+// the newest tag first; the oldest of eight falls off
+__device__ __forceinline__ uint4 set_push(uint4 x, uint32_t tag) {
+    return make_uint4((x.x << 16) | tag, __funnelshift_l(x.x, x.y, 16), __funnelshift_l(x.y, x.z, 16),
+                      __funnelshift_l(x.z, x.w, 16));
+}
+
+// Two candidates per lane that passed the shared-memory table (ids >= 0; -1 =
+// none): both sets are loaded before either is tested, so the warp waits for
+// one round trip.  An id the table holds already becomes -1; the others are
+// added to it.
+__device__ __forceinline__ void l2_filter2(const L2Seen &vt, int32_t &va, int32_t &vb) {
+    uint32_t ta = 0, tb = 0, ia = 0, ib = 0xffffffffu;
+    uint4 xa = make_uint4(0, 0, 0, 0), xb = xa;
+    if (va >= 0) {
+        ia = vt.set_of(va, ta);
+        xa = ld_cg4(vt.sets + ia);
+    }
+    if (vb >= 0) {
+        ib = vt.set_of(vb, tb);
+        xb = ld_cg4(vt.sets + ib);
+    }
+    if (va >= 0) {
+        if (set_has(xa, ta)) {
+            va = -1;
+        } else {
+            xa = set_push(xa, ta);
+            st_cg4(vt.sets + ia, xa);
+            if (ib == ia) xb = xa;  // b's set is the one just written
+        }
+    }
+    if (vb >= 0) {
+        if (set_has(xb, tb)) vb = -1;
+        else st_cg4(vt.sets + ib, set_push(xb, tb));
+    }
+}
+
 // ------------------------------------------------------------ result list --
 // The ef best entries found so far, sorted by (distance, id), in registers:
 // lane l holds positions l*S .. l*S+S-1 of 32*S, and the list takes the last
@@ -430,6 +510,94 @@ struct RegList {
         xm = ((xm & low) | ((xm << 1) & ~(low | bitc)) | (here || pb == 0u ? 0u : bitc)) & kSlots;
     }
 
+    // Merges a chunk's winners - the lanes with win, each (nk, nid) below the
+    // list's last entry when the chunk was taken - into the list at once.
+    // The list after it is the one inserting them one by one would leave:
+    // the best 32*S of the list and the winners, an entry the list holds
+    // already (same id, hence the same traversal distance and key) taken
+    // once with its expanded mark, new entries unexpanded.
+    //   1. the winners are sorted across the lanes (bitonic, 64-bit keys);
+    //   2. the list is staged in shared memory (position p = l*S + s at
+    //      s*32 + l: consecutive lanes, consecutive words) with its marks;
+    //   3. each winner finds its rank r in the list by binary search, and is
+    //      dropped if the entry at r is itself (or the previous winner is);
+    //   4. the j-th kept winner lands at r + j; each lane gathers its S new
+    //      slots: a winner's destination takes that winner, any other slot o
+    //      the list entry at o minus the winners landed before o.
+    // sm: walk_merge_bytes(S) bytes of shared memory, free during the call.
+    __device__ __forceinline__ void merge(bool win, uint32_t nk, uint32_t nid, unsigned char *sm, int lane) {
+        uint64_t *lst = reinterpret_cast<uint64_t *>(sm);  // 32 * S
+        uint64_t *wv = lst + 32 * S;                       // 32 winners
+        uint32_t *dm = reinterpret_cast<uint32_t *>(wv + 32);  // destination masks
+        uint32_t *mk = dm + 32;                             // expanded marks
+        uint64_t x = win ? pack_key(nk, nid) : ~0ull;
+#pragma unroll
+        for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                const uint64_t y = __shfl_xor_sync(kFull, x, j);
+                const bool lower = (lane & j) == 0, up = (lane & kk) == 0;
+                x = (lower == up) == (y < x) ? y : x;
+            }
+        }
+        const int w = __popc(__ballot_sync(kFull, win));
+#pragma unroll
+        for (int s = 0; s < S; s++) lst[s * 32 + lane] = pack_key(k[s], id[s]);
+        mk[lane] = xm;
+        dm[lane] = 0u;
+        const uint64_t prev = __shfl_up_sync(kFull, x, 1);
+        __syncwarp();
+        bool keep = lane < w && (lane == 0 || prev != x);
+        int r = 0;
+        if (keep) {
+            int lo = 0, hi = 32 * S;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (lst[(mid % S) * 32 + mid / S] < x) lo = mid + 1;
+                else hi = mid;
+            }
+            r = lo;
+            if (r < 32 * S && lst[(r % S) * 32 + r / S] == x) keep = false;
+        }
+        const unsigned km = __ballot_sync(kFull, keep);
+        if (km == 0u) return;
+        const int dst = r + __popc(km & ((1u << lane) - 1u));
+        if (keep) {
+            wv[__popc(km & ((1u << lane) - 1u))] = x;
+            if (dst < 32 * S) atomicOr(dm + dst / S, 1u << (dst % S));
+        }
+        __syncwarp();
+        const uint32_t my = dm[lane];
+        // winners landing before this lane's first slot
+        int before = __popc(my);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, before, o);
+            if (lane >= o) before += t;
+        }
+        before -= __popc(my);
+        uint32_t nm = 0u;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            uint64_t v;
+            uint32_t mark;
+            if ((my >> s) & 1u) {
+                v = wv[before];
+                mark = 0u;
+                before++;
+            } else {
+                const int p = lane * S + s - before;
+                v = lst[(p % S) * 32 + p / S];
+                mark = (mk[p / S] >> (p % S)) & 1u;
+            }
+            k[s] = (uint32_t)(v >> 32);
+            id[s] = (uint32_t)v;
+            nm |= mark << s;
+        }
+        xm = nm & kSlots;
+        __syncwarp();
+    }
+
     // Marks the first expandable entry as expanded and returns its id, or -1
     // if there is none.
     __device__ __forceinline__ int32_t take_first(int lane) {
@@ -498,7 +666,7 @@ __global__ void __maxnreg__(walk_max_regs(TRAV, S, EXP))
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const WalkLayout lay = walk_layout(a.rb, a.trav_row_bytes, a.tq_row_bytes, a.hlog2, a.tag16 != 0);
+    const WalkLayout lay = walk_layout(a.rb, a.trav_row_bytes, a.tq_row_bytes, a.hlog2, a.tag16 != 0, S);
     unsigned char *my = smem + (size_t)wib * lay.total;
     SeenTable seen;
     seen.w = reinterpret_cast<uint32_t *>(my + lay.tab);
@@ -515,6 +683,13 @@ __global__ void __maxnreg__(walk_max_regs(TRAV, S, EXP))
     __syncwarp();
     uint8_t *qbuf = my + lay.qbuf;
     RowFetch f{my + lay.rowbuf, (int32_t)lay.stride, bar, 0u};
+    L2Seen vt;
+    vt.nsets = 1 << a.vt_log2sets;
+    vt.sets = a.vt ? reinterpret_cast<uint4 *>(a.vt) +
+                         ((int64_t)(blockIdx.x * (blockDim.x >> 5) + wib) << a.vt_log2sets)
+                   : nullptr;
+    vt.bmask = a.vt_bmask;
+    vt.tbits = a.vt_tbits;
 
     const TravView tv{a.trav, a.trav_zero, (int32_t)a.trav_row_bytes};
     const bool ip = gp->metric == PK_METRIC_IP;
@@ -617,6 +792,8 @@ __global__ void __maxnreg__(walk_max_regs(TRAV, S, EXP))
         uint64_t wk = pack_key(kEmpty, kEmpty);
         if (!failed) {
             seen.clear(lane);
+            if (vt.sets)
+                for (int i = lane; i < vt.nsets; i += 32) st_cg4(vt.sets + i, make_uint4(0, 0, 0, 0));
             __syncwarp();
             if (enter < 0 || enter >= lim0) enter = 0;
             if (lane == 0) crow[0] = enter;
@@ -626,7 +803,14 @@ __global__ void __maxnreg__(walk_max_regs(TRAV, S, EXP))
             trav_dist_buf<TRAV>(ip, qnorm, qfac, f, tdb, qbuf, cd, 1, lane);
             const float d0 = cd[0];
             list.put_first(L, dist_key(d0), (uint32_t)enter, lane);
-            if (lane == 0) seen.test_and_mark(enter);
+            if (lane == 0) {
+                seen.test_and_mark(enter);
+                if (vt.sets) {
+                    uint32_t tag;
+                    uint4 *p = vt.sets + vt.set_of(enter, tag);
+                    st_cg4(p, set_push(ld_cg4(p), tag));
+                }
+            }
             __syncwarp();
             wk = list.last();
         }
@@ -645,6 +829,13 @@ __global__ void __maxnreg__(walk_max_regs(TRAV, S, EXP))
                     ok = nd < kInf;
                 }
                 unsigned m = __ballot_sync(kFull, ok && pack_key(nk, nid) < wk);
+                if constexpr (S >= kMergeMinSlots) {
+                    if (__popc(m) >= a.merge_min) {
+                        list.merge((m >> lane) & 1u, nk, nid, f.buf, lane);
+                        wk = list.last();
+                        m = 0u;
+                    }
+                }
                 while (m) {
                     const int src = __ffs(m) - 1;
                     m &= m - 1;
@@ -687,15 +878,28 @@ __global__ void __maxnreg__(walk_max_regs(TRAV, S, EXP))
                 const int64_t base = (int64_t)pc[p] * cap0;
                 cnt[3]++;
                 cnt[5] += deg;
-                for (int j0 = 0; j0 < deg; j0 += 32) {
-                    const int j = j0 + lane;
-                    int32_t v = -1;
-                    if (j < deg) v = (j < cap0 && j0 == 0) ? pa0[p] : (j < cap0 && j0 == 32) ? pa1[p] : L0.adj[base + j];
-                    const bool fresh = v >= 0 && v < lim0 && seen.test_and_mark(v);
-                    if (!append_pending(fresh, v, v, crow, cid, n, rb, lane, flush0)) {
-                        failed = true;
-                        break;
+                // 64 neighbour slots at a time, two per lane: the shared-memory
+                // table first, then (for what it does not hold) the table in
+                // L2, both sets loaded before either is tested
+                for (int j0 = 0; j0 < deg; j0 += 64) {
+                    const int ja = j0 + lane, jb = ja + 32;
+                    int32_t va = -1, vb = -1;
+                    if (ja < deg) va = (j0 == 0 && ja < cap0) ? pa0[p] : L0.adj[base + ja];
+                    if (jb < deg) vb = (j0 == 0 && jb < cap0) ? pa1[p] : L0.adj[base + jb];
+                    if (!(va >= 0 && va < lim0 && seen.test_and_mark(va))) va = -1;
+                    if (!(vb >= 0 && vb < lim0 && seen.test_and_mark(vb))) vb = -1;
+                    if (vt.sets) l2_filter2(vt, va, vb);
+                    // one site appends (and flushes) both halves: the flush's
+                    // code is inlined once here
+#pragma unroll 1
+                    for (int h2 = 0; h2 < 2 && j0 + 32 * h2 < deg; h2++) {
+                        const int32_t v = h2 == 0 ? va : vb;
+                        if (!append_pending(v >= 0, v, v, crow, cid, n, rb, lane, flush0)) {
+                            failed = true;
+                            break;
+                        }
                     }
+                    if (failed) break;
                 }
             }
             if (!failed && n > 0 && !flush0(n)) failed = true;

@@ -41,7 +41,36 @@ struct WalkArgs {
     int64_t trav_row_bytes;
     int64_t trav_rows;          // rows in the traversal copy; node ids stay below it
     int64_t trav_data_bytes;    // the values of a row; E4M3 L2 rows have their norm after them (float)
+    // second level of the visited filter: per warp (blockIdx.x * warps per
+    // block + warp) 2^vt_log2sets sets of eight 16-bit tags in global memory,
+    // small enough to stay in L2; null = the shared-memory table alone
+    void *vt;
+    int32_t vt_log2sets;
+    int32_t vt_tbits;           // tag bits: the id's bits beyond the set index (<= 15)
+    uint32_t vt_bmask;          // 2^(vt_log2sets + vt_tbits) - 1
+    // a batch's winners (candidates below the list's last entry) are merged
+    // into the list at once when at least merge_min of a 32-candidate chunk
+    // win (lists of kMergeMinSlots or more slots), else inserted one by one
+    int32_t merge_min;
 };
+
+// Sets (of eight 16-bit tags, 16 bytes) of a walk warp's visited table in
+// global memory for lists of `slots` per lane over `ids` node ids.  A walk at
+// ef meets about 1.5k + 16 ef distinct nodes on 128-dimensional data with
+// 64 neighbours per node; the table holds about 1.25x that for the widest
+// ef of the width (8-way sets: few overflow), at most twice the ids, and at
+// least enough sets that the tag (the id's remaining bits) fits in 15 bits.
+__host__ __device__ inline int visited_log2sets(int slots, int64_t ids) {
+    const int64_t cap = 32 * (int64_t)slots;
+    int64_t want = (1536 + 16 * cap) * 5 / 4;
+    if (want > 2 * ids) want = 2 * ids;
+    int l = 0;
+    while (((int64_t)8 << l) < want) l++;
+    int b = 1;
+    while (b < 32 && ((int64_t)1 << b) < ids) b++;
+    if (b - l > 15) l = b - 15;
+    return l;
+}
 
 // Shared-memory stride of a staged traversal row: the row padded to an odd
 // number of 16-byte chunks, so that 8 consecutive rows start in 8 different
@@ -62,20 +91,39 @@ __host__ __device__ inline bool seen_tag16(int64_t n, int hlog2) {
     return b - (hlog2 - 2) <= 15;
 }
 
-// Shared memory of one walk warp: the staged rows (rb rows, stride apart),
-// the query in the traversal format, the recently-seen table, the pending batch
-// (rows, ids, distances), the mbarrier.  Every region starts on a 16-byte
-// boundary (bulk copies land on 16-byte boundaries).
+// Lists of at least this many slots per lane merge a batch's winning
+// candidates into the list at once when there are enough of them (one merge
+// costs about as much as two or three one-at-a-time insertions at 16 slots).
+constexpr int kMergeMinSlots = 6;
+
+// Default winners of a chunk from which a list of `slots` per lane merges
+// them at once (below it, one-by-one insertions are cheaper).
+__host__ __device__ inline int merge_min_for(int slots) { return slots >= 12 ? 3 : slots >= 8 ? 4 : 5; }
+
+// Shared memory the merge works in: the list (32 * slots packed entries), the
+// winners (32 packed), the destination masks and the expanded marks (32 words
+// each).  It reuses the staged rows' space, which is free between a batch's
+// distances and the next fetch.
+__host__ __device__ inline int64_t walk_merge_bytes(int slots) {
+    return slots >= kMergeMinSlots ? 8 * 32 * (int64_t)slots + 8 * 32 + 4 * 32 + 4 * 32 : 0;
+}
+
+// Shared memory of one walk warp: the staged rows (rb rows, stride apart; at
+// least the merge's working space for the list width), the query in the
+// traversal format, the recently-seen table, the pending batch (rows, ids,
+// distances), the mbarrier.  Every region starts on a 16-byte boundary (bulk
+// copies land on 16-byte boundaries).
 struct WalkLayout {
     int rowbuf, qbuf, tab, crow, cid, cd, bar, total;
     int64_t stride;
 };
 __host__ __device__ inline WalkLayout walk_layout(int rb, int64_t trav_row_bytes, int64_t query_bytes, int hlog2,
-                                                  bool tag16) {
+                                                  bool tag16, int slots) {
     WalkLayout w;
     w.stride = stage_stride(trav_row_bytes);
     w.rowbuf = 0;
-    w.qbuf = align16((int64_t)rb * w.stride);
+    const int64_t rows = (int64_t)rb * w.stride, mb = walk_merge_bytes(slots);
+    w.qbuf = align16(rows > mb ? rows : mb);
     w.tab = w.qbuf + align16(query_bytes);
     w.crow = w.tab + ((tag16 ? 2 : 4) << hlog2);
     w.cid = w.crow + align16(4 * (int64_t)rb);

@@ -121,6 +121,12 @@ struct FastCtx {
     int64_t fq_n = 0, tq_n = 0;
     float *d_qn = nullptr;
     int64_t qn_n = 0;
+    // the walk's visited tables in L2 (per warp of each width's launch);
+    // a context with vt_fixed never allocates them (it uses what d_vt holds,
+    // or runs with the shared-memory table alone)
+    uint8_t *d_vt = nullptr;
+    int64_t vt_n = 0;
+    bool vt_fixed = false;
     // optional timing of the last launch: before the walk, after it, after
     // the re-rank (created on first use)
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
@@ -199,6 +205,12 @@ struct pk_index {
     // above for that class's launch (0 = none)
     int cls_rb[pk::kSlotClasses] = {}, cls_hlog2[pk::kSlotClasses] = {}, cls_wpb[pk::kSlotClasses] = {};
     bool fast_timing = false;      // record events around the walk and the re-rank
+    // the walk's visited tables in L2: 0 = sized by list width, -1 = off,
+    // > 0 = log2 of the sets for every width
+    int fast_vt = 0;
+    // winners of a 32-candidate chunk from which the walk merges them into a
+    // wide list at once: 0 = by list width, -1 = never (one by one)
+    int fast_merge = 0;
 
     size_t dev_bytes = 0;
 
@@ -860,10 +872,11 @@ int walk_shape(const pk_index *h, WalkShape &w, int cls = -1) {
     w.tag16 = pk::seen_tag16(ids, w.hlog2);
     w.idbits = std::max(pk::idbits_for(ids), w.hlog2 - 2);
     const int64_t qb = pk::trav_query_bytes(h->trav, h->trav_data_bytes);
-    w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, qb, w.hlog2, w.tag16).total;
+    const int sl = pk::slot_class_width(cls >= 0 && cls < pk::kSlotClasses ? cls : pk::kSlotClasses - 1);
+    w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, qb, w.hlog2, w.tag16, sl).total;
     while (w.wpb > 1 && w.smem > 200 * 1024) {
         w.wpb /= 2;
-        w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, qb, w.hlog2, w.tag16).total;
+        w.smem = (size_t)w.wpb * pk::walk_layout(w.rb, trb, qb, w.hlog2, w.tag16, sl).total;
     }
     if (w.smem > 227 * 1024) return fail(PK_ERR_ARG, "walk working set exceeds shared memory: lower rows or filter bits");
     return PK_OK;
@@ -921,6 +934,39 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     a.trav_row_bytes = h->trav_row_bytes;
     a.trav_data_bytes = h->trav_data_bytes;
     a.trav_rows = h->trav_rows;
+    // each width's launch shape, grid and visited tables in L2 (one table
+    // per warp of every width's launch: the launches run side by side)
+    struct ClsPlan {
+        WalkShape ws;
+        int64_t grid = 0, vt_off = 0;
+        int vt_log2 = 0;
+    } plan[pk::kSlotClasses];
+    int64_t vt_total = 0;
+    const int64_t ids0 = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
+    for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
+        const int sl = pk::slot_class_width(cls);
+        if (!binned && sl != slots) continue;
+        ClsPlan &P = plan[cls];
+        PK_TRY(walk_shape(h, P.ws, cls));
+        const int nb = pk::walk_blocks_per_sm(h->trav, sl, a.expand, P.ws.wpb, P.ws.smem);
+        if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
+        P.grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + P.ws.wpb - 1) / P.ws.wpb);
+        if (h->fast_vt >= 0) {
+            int l = h->fast_vt > 0 ? h->fast_vt : pk::visited_log2sets(sl, ids0);
+            l = std::max(l, pk::idbits_for(ids0) - 15);
+            P.vt_log2 = l;
+            P.vt_off = vt_total;
+            vt_total += P.grid * P.ws.wpb * ((int64_t)16 << l);
+        }
+    }
+    // the tables are scratch of the walk's own: if they cannot be had, the
+    // walk runs with the shared-memory table alone (same results)
+    if (vt_total > c.vt_n || !c.d_vt) {
+        if (c.vt_fixed || ensure_buf(h, &c.d_vt, c.vt_n, vt_total) != PK_OK) {
+            if (!c.vt_fixed) c.vt_n = 0;
+            vt_total = 0;
+        }
+    }
     const bool timed = h->fast_timing && &c == &h->fctx;
     if (timed) {
         for (cudaEvent_t &e : c.ev)
@@ -934,6 +980,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
         const int sl = pk::slot_class_width(cls);
         if (!binned && sl != slots) continue;
+        const ClsPlan &P = plan[cls];
         cudaStream_t ls = s;
         if (binned) {
             if (!c.aux[cls]) PK_CUDA(cudaStreamCreateWithFlags(&c.aux[cls], cudaStreamNonBlocking));
@@ -941,18 +988,20 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
             ls = c.aux[cls];
             PK_CUDA(cudaStreamWaitEvent(ls, c.fork, 0));
         }
-        PK_TRY(walk_shape(h, ws, cls));
-        a.rb = ws.rb;
-        a.hlog2 = ws.hlog2;
-        a.tag16 = ws.tag16 ? 1 : 0;
-        a.idbits = ws.idbits;
-        const int nb = pk::walk_blocks_per_sm(h->trav, sl, a.expand, ws.wpb, ws.smem);
-        if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
-        const int64_t grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + ws.wpb - 1) / ws.wpb);
+        a.rb = P.ws.rb;
+        a.hlog2 = P.ws.hlog2;
+        a.tag16 = P.ws.tag16 ? 1 : 0;
+        a.idbits = P.ws.idbits;
+        a.vt = vt_total > 0 ? c.d_vt + P.vt_off : nullptr;
+        a.vt_log2sets = P.vt_log2;
+        const int vb = std::max(pk::idbits_for(ids0), P.vt_log2);
+        a.vt_tbits = vb - P.vt_log2;
+        a.vt_bmask = vb >= 32 ? 0xffffffffu : (1u << vb) - 1u;
+        a.merge_min = h->fast_merge < 0 ? (1 << 30) : h->fast_merge > 0 ? h->fast_merge : pk::merge_min_for(sl);
         a.work = c.d_work + kWorkCounters + cls;
         a.qlist = binned ? c.d_lists + cls * nq : nullptr;
         a.qcount = binned ? c.d_work + kWorkCounts + cls : nullptr;
-        PK_CUDA(pk::launch_walk(h->dg, h->trav, sl, a, (int)grid, ws.wpb, ws.smem, ls));
+        PK_CUDA(pk::launch_walk(h->dg, h->trav, sl, a, (int)P.grid, P.ws.wpb, P.ws.smem, ls));
         if (binned) {
             PK_CUDA(cudaEventRecord(c.join[cls], ls));
             PK_CUDA(cudaStreamWaitEvent(s, c.join[cls], 0));
@@ -1047,6 +1096,7 @@ void free_fast_ctx(pk_index *h, FastCtx &c) {
     dfree(h, c.d_fq, (size_t)c.fq_n);
     dfree(h, c.d_tq, (size_t)c.tq_n);
     dfree(h, c.d_qn, 4 * (size_t)c.qn_n);
+    if (!c.vt_fixed) dfree(h, c.d_vt, (size_t)c.vt_n);
     c = FastCtx{};
 }
 
@@ -1969,6 +2019,7 @@ void srv_loop(pk_server *S) {
                 int32_t *d_ids = reinterpret_cast<int32_t *>(base + L.ids);
                 float *d_d = reinterpret_cast<float *>(base + L.d);
                 // the search's scratch, in the chunk (sized so that nothing grows)
+                sl.ctx.vt_fixed = true;
                 sl.ctx.d_work = reinterpret_cast<int32_t *>(base + L.work);
                 sl.ctx.work_n = kWorkInts;
                 sl.ctx.d_cand = reinterpret_cast<int32_t *>(base + L.cand);
@@ -2405,6 +2456,20 @@ int pk_index_tune_fast_classes(pk_index *h, const void *queries, int64_t nq, int
     } catch (...) {
         return fail(PK_ERR_STATE, "pk_index_tune_fast_classes: unexpected exception");
     }
+}
+
+int pk_index_set_fast_visited(pk_index *h, int32_t log2_sets) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    if (log2_sets < -1 || log2_sets > 20) return fail(PK_ERR_ARG, "log2_sets must be -1, 0 or 1..20");
+    h->fast_vt = log2_sets;
+    return PK_OK;
+}
+
+int pk_index_set_fast_merge(pk_index *h, int32_t min_winners) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    if (min_winners < -1 || min_winners > 32) return fail(PK_ERR_ARG, "min_winners must be -1, 0 or 1..32");
+    h->fast_merge = min_winners;
+    return PK_OK;
 }
 
 int pk_index_set_fast_timing(pk_index *h, int enable) {

@@ -66,15 +66,23 @@ int main() {
                 for (int rb : {1, 8, 16, 24, 32, 48, 64, 256}) {
                     for (int hl = 5; hl <= 15; hl++) {
                         for (bool t16 : {false, true}) {
-                            const WalkLayout w = walk_layout(rb, trb, qb, hl, t16);
+                          for (int c = 0; c < kSlotClasses; c++) {
+                            const int sl = slot_class_width(c);
+                            const WalkLayout w = walk_layout(rb, trb, qb, hl, t16, sl);
                             CHECK(w.stride == st, "stride");
                             CHECK(w.qbuf >= rb * st && w.qbuf % 16 == 0, "qbuf %d", w.qbuf);
+                            // the merge's working space (list, winners, masks,
+                            // marks) fits in the staged rows' region
+                            CHECK(w.qbuf >= walk_merge_bytes(sl), "merge space %d for %d slots", w.qbuf, sl);
+                            CHECK(sl < kMergeMinSlots || walk_merge_bytes(sl) >= 8 * 32 * sl + 8 * 32 + 8 * 32,
+                                  "merge bytes %lld", (long long)walk_merge_bytes(sl));
                             CHECK(w.tab >= w.qbuf + qb && w.tab % 16 == 0, "tab %d", w.tab);
                             CHECK(w.crow >= w.tab + ((t16 ? 2 : 4) << hl) && w.crow % 16 == 0, "crow %d", w.crow);
                             CHECK(w.cid >= w.crow + 4 * rb && w.cid % 16 == 0, "cid %d", w.cid);
                             CHECK(w.cd >= w.cid + 4 * rb && w.cd % 16 == 0, "cd %d", w.cd);
                             CHECK(w.bar >= w.cd + 4 * rb && w.bar % 16 == 0, "bar %d", w.bar);
                             CHECK(w.total >= w.bar + 8, "total %d", w.total);
+                          }
                         }
                     }
                 }
@@ -92,6 +100,22 @@ int main() {
                                          (long long)n, hl);
         }
     }
+    // visited tables in L2: exact tags (the id's bits beyond the set index fit
+    // 15 bits, so tag + 1 fits 16), at most about twice the ids, and room
+    // for what a walk of the width meets
+    for (int c = 0; c < kSlotClasses; c++) {
+        const int sl = slot_class_width(c);
+        for (int64_t n : {2LL, 100LL, 3000LL, 1LL << 16, 1000000LL, 10000000LL, 1LL << 28, 1LL << 31}) {
+            const int l = visited_log2sets(sl, n);
+            const int b = idbits_for(n) > l ? idbits_for(n) : l;
+            CHECK(l >= 0 && l <= 20, "log2 sets %d", l);
+            CHECK(b - l <= 15, "tag bits %d (n %lld, slots %d)", b - l, (long long)n, sl);
+            CHECK(((int64_t)8 << l) >= ((1536 + 16 * 32 * (int64_t)sl) * 5 / 4 < 2 * n ? (1536 + 16 * 32 * sl) * 5 / 4 : 2 * n),
+                  "table too small: 2^%d sets (n %lld, slots %d)", l, (long long)n, sl);
+            CHECK(l == 0 || ((int64_t)8 << (l - 1)) < 2 * n || b - (l - 1) > 15, "table larger than needed");
+        }
+    }
+    for (int s = 1; s <= 32; s++) CHECK(merge_min_for(s) >= 1 && merge_min_for(s) <= 32, "merge_min %d", s);
     std::printf("ok\n");
     return 0;
 }

@@ -237,3 +237,61 @@ def test_seen_table_layouts_agree(gpu):
     np.testing.assert_array_equal(a_d, b_d)
     gt, _ = datasets.exact_knn(base, queries, 10, "ip")
     assert datasets.recall_at_k(a_i, gt, 10) >= 0.9
+
+
+# (log2 of the L2 visited table's sets, merge threshold): the table off, by
+# width, or eight sets (it forgets most ids); one-by-one insertions only,
+# merges by width, or a merge for every chunk with a winner
+WALK_VARIANTS = [(-1, 1), (0, 0), (0, 1), (3, 0), (0, 32)]
+
+
+@pytest.mark.parametrize("trav", ["f16", "fp8"])
+def test_fast_visited_tables_and_merges_keep_results(trav, gpu):
+    """The walk's second-level visited table (in L2) and its batched merge of a
+    chunk's winners into wide lists change the work, not the answer: every
+    variant returns what the walk with the shared-memory table alone and
+    one-by-one insertions returns, for per-query ef over every list width (up
+    to 1024), with a small shared-memory table so that ids are forgotten and met
+    again."""
+    import torch
+    base, queries = datasets.gmm_f16(20000, 600, 64, ncomp=24, sigma=0.5, seed=11)
+    idx = HNSWIndex(64, np.float16, "l2", M=16, ef_construction=100)
+    idx.set_seed(11)
+    idx.build(base)
+    idx.prepare_fast(trav)
+    rng = np.random.default_rng(12)
+    nq = len(queries)
+    ks = rng.choice([1, 10, 100], size=nq).astype(np.int32)
+    efs = np.array([rng.integers(max(16, int(k)), 1025) for k in ks], np.int32)
+    stride = int(ks.max())
+    q = torch.from_numpy(queries).cuda()
+    kd, ed = torch.from_numpy(ks).cuda(), torch.from_numpy(efs).cuda()
+
+    def run():
+        ids = torch.full((nq, stride), -7, dtype=torch.int32, device="cuda")
+        ds = torch.zeros((nq, stride), dtype=torch.float32, device="cuda")
+        idx.search_fast_device(q, stride, int(efs.max()), ids, ds, k_per_query=kd, ef_per_query=ed)
+        torch.cuda.synchronize()
+        return ids.cpu().numpy(), ds.cpu().numpy()
+
+    idx.set_fast_params(8, 5, 2)
+    idx.set_fast_visited(-1)
+    idx.set_fast_merge(-1)
+    want_i, want_d = run()
+    for i in range(nq):
+        _valid_rows(want_i[i:i + 1, :ks[i]], want_d[i:i + 1, :ks[i]])
+    gt, _ = datasets.exact_knn(base, queries, 10, "l2")
+    assert datasets.recall_at_k(want_i[:, :10][ks >= 10], gt[ks >= 10], 10) >= 0.9
+    for vt, merge in WALK_VARIANTS:
+        idx.set_fast_visited(vt)
+        idx.set_fast_merge(merge)
+        got_i, got_d = run()
+        np.testing.assert_array_equal(got_i, want_i, err_msg=f"visited {vt}, merge {merge}")
+        np.testing.assert_array_equal(got_d, want_d, err_msg=f"visited {vt}, merge {merge}")
+    # the tuned shapes too
+    idx.set_fast_params()
+    idx.set_fast_visited(0)
+    idx.set_fast_merge(0)
+    got_i, got_d = run()
+    np.testing.assert_array_equal(got_i, want_i)
+    np.testing.assert_array_equal(got_d, want_d)
