@@ -247,7 +247,13 @@ int pk_index_set_fast_class_params(pk_index *h, int32_t width_class, int32_t row
  * whole arena is refused at submission with PK_ERR_CAPACITY.  The arena is
  * device_bytes (pk_server_create_with_memory) or, for pk_server_create, enough
  * for every stream's full batch at max_k and max_ef but at most half of the
- * device memory free at creation.  Each result equals what
+ * device memory free at creation; pk_server_create also gives each stream the
+ * walk's visited tables in L2 (pk_index_set_fast_visited) for a full batch at
+ * max_ef, outside the arena, where they can be allocated (without them a
+ * stream's batches return the same results, more slowly), while
+ * pk_server_create_with_memory with device_bytes > 0 takes device_bytes and
+ * nothing more (device_bytes = 0: as pk_server_create).  Each
+ * result equals what
  * pk_index_search_fast returns for that request alone.  A batch that does not
  * finish within the watchdog period (30 s) fails its requests with
  * PK_ERR_TIMEOUT.  The index must not be modified while a server uses it.

@@ -882,6 +882,36 @@ int walk_shape(const pk_index *h, WalkShape &w, int cls = -1) {
     return PK_OK;
 }
 
+// One walk launch per list width: its shape, grid and visited tables in L2
+// (one table per warp of every width's launch, since the launches run side
+// by side; vt_off into one buffer of vt_total bytes, 0 with the tables off).
+struct ClsPlan {
+    WalkShape ws;
+    int64_t grid = 0, vt_off = 0;
+    int vt_log2 = 0;
+};
+int walk_plan(pk_index *h, int64_t nq, int slots, bool binned, int expand, ClsPlan *plan, int64_t &vt_total) {
+    vt_total = 0;
+    const int64_t ids0 = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
+    for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
+        const int sl = pk::slot_class_width(cls);
+        if (!binned && sl != slots) continue;
+        ClsPlan &P = plan[cls];
+        PK_TRY(walk_shape(h, P.ws, cls));
+        const int nb = pk::walk_blocks_per_sm(h->trav, sl, expand, P.ws.wpb, P.ws.smem);
+        if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
+        P.grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + P.ws.wpb - 1) / P.ws.wpb);
+        if (h->fast_vt >= 0) {
+            int l = h->fast_vt > 0 ? h->fast_vt : pk::visited_log2sets(sl, ids0);
+            l = std::max(l, pk::idbits_for(ids0) - 15);
+            P.vt_log2 = l;
+            P.vt_off = vt_total;
+            vt_total += P.grid * P.ws.wpb * ((int64_t)16 << l);
+        }
+    }
+    return PK_OK;
+}
+
 // Low-precision walk, then exact re-rank of each query's final list.  Fully
 // asynchronous on stream s.
 int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_queries, int64_t nq, int32_t k,
@@ -934,34 +964,12 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     a.trav_row_bytes = h->trav_row_bytes;
     a.trav_data_bytes = h->trav_data_bytes;
     a.trav_rows = h->trav_rows;
-    // each width's launch shape, grid and visited tables in L2 (one table
-    // per warp of every width's launch: the launches run side by side)
-    struct ClsPlan {
-        WalkShape ws;
-        int64_t grid = 0, vt_off = 0;
-        int vt_log2 = 0;
-    } plan[pk::kSlotClasses];
+    ClsPlan plan[pk::kSlotClasses];
     int64_t vt_total = 0;
-    const int64_t ids0 = std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows));
-    for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
-        const int sl = pk::slot_class_width(cls);
-        if (!binned && sl != slots) continue;
-        ClsPlan &P = plan[cls];
-        PK_TRY(walk_shape(h, P.ws, cls));
-        const int nb = pk::walk_blocks_per_sm(h->trav, sl, a.expand, P.ws.wpb, P.ws.smem);
-        if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
-        P.grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + P.ws.wpb - 1) / P.ws.wpb);
-        if (h->fast_vt >= 0) {
-            int l = h->fast_vt > 0 ? h->fast_vt : pk::visited_log2sets(sl, ids0);
-            l = std::max(l, pk::idbits_for(ids0) - 15);
-            P.vt_log2 = l;
-            P.vt_off = vt_total;
-            vt_total += P.grid * P.ws.wpb * ((int64_t)16 << l);
-        }
-    }
+    PK_TRY(walk_plan(h, nq, slots, binned, a.expand, plan, vt_total));
     // the tables are scratch of the walk's own: if they cannot be had, the
     // walk runs with the shared-memory table alone (same results)
-    if (vt_total > c.vt_n || !c.d_vt) {
+    if (vt_total > 0 && (vt_total > c.vt_n || !c.d_vt)) {
         if (c.vt_fixed || ensure_buf(h, &c.d_vt, c.vt_n, vt_total) != PK_OK) {
             if (!c.vt_fixed) c.vt_n = 0;
             vt_total = 0;
@@ -994,7 +1002,8 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
         a.idbits = P.ws.idbits;
         a.vt = vt_total > 0 ? c.d_vt + P.vt_off : nullptr;
         a.vt_log2sets = P.vt_log2;
-        const int vb = std::max(pk::idbits_for(ids0), P.vt_log2);
+        const int vb = std::max(pk::idbits_for(std::max<int64_t>(2, std::min<int64_t>(h->hg.L[0].lcap, h->trav_rows))),
+                                P.vt_log2);
         a.vt_tbits = vb - P.vt_log2;
         a.vt_bmask = vb >= 32 ? 0xffffffffu : (1u << vb) - 1u;
         a.merge_min = h->fast_merge < 0 ? (1 << 30) : h->fast_merge > 0 ? h->fast_merge : pk::merge_min_for(sl);
@@ -1782,6 +1791,10 @@ struct SrvSlot {
     int32_t nq = 0, stride = 0;
     size_t chunk_off = 0, chunk_bytes = 0;  // the batch's arena chunk
     Clock::time_point t_launch;
+    // the walk's visited tables in L2 for this slot's batches (outside the
+    // arena; null = the walk runs with its shared-memory table alone)
+    uint8_t *vt = nullptr;
+    size_t vt_bytes = 0;
 };
 
 }  // namespace
@@ -2019,7 +2032,6 @@ void srv_loop(pk_server *S) {
                 int32_t *d_ids = reinterpret_cast<int32_t *>(base + L.ids);
                 float *d_d = reinterpret_cast<float *>(base + L.d);
                 // the search's scratch, in the chunk (sized so that nothing grows)
-                sl.ctx.vt_fixed = true;
                 sl.ctx.d_work = reinterpret_cast<int32_t *>(base + L.work);
                 sl.ctx.work_n = kWorkInts;
                 sl.ctx.d_cand = reinterpret_cast<int32_t *>(base + L.cand);
@@ -2098,6 +2110,7 @@ void srv_free(pk_server *S) {
         cudaFreeHost(sl.h_status);
         if (sl.ev) cudaEventDestroy(sl.ev);
         if (sl.stream) cudaStreamDestroy(sl.stream);
+        dfree(S->h, sl.vt, sl.vt_bytes);
     }
     if (S->arena) dfree(S->h, S->arena, S->arena_bytes);
     delete S;
@@ -2157,6 +2170,26 @@ int srv_create(pk_server **out, pk_index *h, int traversal, int nslots, int32_t 
             return fail(PK_ERR_OOM, "server host buffers could not be allocated");
         }
     }
+    // with the default arena, each slot also gets the walk's visited tables
+    // for a full batch at the largest ef (a batch whose launch shapes need
+    // more, or a slot whose tables could not be allocated, walks with the
+    // shared-memory table alone: the same results); an explicit device_bytes
+    // is all the device memory the server takes
+    if (device_bytes == 0) {
+        ClsPlan plan[pk::kSlotClasses];
+        int64_t vt_total = 0;
+        if (walk_plan(h, max_batch, pk::list_slots(max_ef), true, S->expand, plan, vt_total) == PK_OK &&
+            vt_total > 0) {
+            for (SrvSlot &sl : S->slots) {
+                if (dalloc(h, (void **)&sl.vt, (size_t)vt_total) != PK_OK) break;
+                sl.vt_bytes = (size_t)vt_total;
+                sl.ctx.d_vt = sl.vt;
+                sl.ctx.vt_n = vt_total;
+            }
+        }
+        cudaGetLastError();
+    }
+    for (SrvSlot &sl : S->slots) sl.ctx.vt_fixed = true;
     S->worker = std::thread(srv_loop, S);
     *out = S;
     return PK_OK;
