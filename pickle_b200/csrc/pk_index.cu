@@ -985,9 +985,13 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
         if (!c.fork) PK_CUDA(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
         PK_CUDA(cudaEventRecord(c.fork, s));
     }
-    for (int cls = 0; cls < pk::kSlotClasses && pk::slot_class_width(cls) <= slots; cls++) {
+    // widest first: each launch fills the GPU and the next one's blocks take
+    // the SMs its warps leave as its work runs out, so the launch that ends
+    // the batch - whose tail nothing fills - is the one with the shortest
+    // queries
+    for (int cls = pk::kSlotClasses - 1; cls >= 0; cls--) {
         const int sl = pk::slot_class_width(cls);
-        if (!binned && sl != slots) continue;
+        if (sl > slots || (!binned && sl != slots)) continue;
         const ClsPlan &P = plan[cls];
         cudaStream_t ls = s;
         if (binned) {
@@ -1526,7 +1530,8 @@ static int pk_index_prepare_fast_impl(pk_index *h, int traversal) {
 // and returns the fastest.  The result lists are the same for every shape;
 // only the work and its overlap change, so the choice is by time alone.  The
 // shapes are tried as the shape of ef's list-width class, which is left as it
-// was.  reps = timed runs per shape (after one warm-up run).
+// was.  reps = timed runs per shape (after one warm-up run); a shape's time is
+// the fastest of them (the least disturbed by whatever else shares the GPU).
 int tune_shape(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t expand, int reps,
                cudaStream_t s, int &brb, int &bh, int &bw, float &best) {
     PK_TRY(ensure_buf(h, &h->d_fids, h->fids_n, nq * k));
@@ -1560,12 +1565,11 @@ int tune_shape(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t 
             float t = 0.f;
             if (rc == PK_OK && cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
                 rc = fail(PK_ERR_CUDA, "cudaEventElapsedTime failed");
-            if (rep > 0) ms += t;
+            if (rep > 0) ms = rep == 1 ? t : std::min(ms, t);
         }
         // a walk that stopped early on a fetch timeout must not look fast
         if (rc == PK_OK) rc = fast_status(h, h->fctx, s);
         if (rc != PK_OK) return false;
-        ms /= (float)reps;
         if (best < 0.f || ms < best) {
             best = ms;
             brb = rb;
@@ -1579,7 +1583,9 @@ int tune_shape(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t 
     // as ef grows, and the staged rows share the same shared memory: large
     // rows at 32 per batch leave room only for small tables); stage 2: rows
     // per batch at the best triple
-    const int hls[] = {8, 9, 10, 11, 12, 13};
+    // (with the visited tables in L2 behind it, small shared-memory tables
+    // that leave room for more warps are often the fastest)
+    const int hls[] = {6, 8, 9, 10, 11, 12, 13};
     const int wps[] = {1, 2, 4};
     const int rbs1[] = {16, 32};
     for (int rb : rbs1)
@@ -1644,7 +1650,7 @@ static int pk_index_tune_fast_classes_impl(pk_index *h, const void *queries, int
         const int ef = std::min(32 * pk::slot_class_width(c), std::min(max_ef, pk::kFastMaxEf));
         int rb = 0, hl = 0, wp = 0;
         float ms = 0.f;
-        PK_TRY(tune_shape(h, queries, nq, std::min(k, ef), ef, expand, 1, static_cast<cudaStream_t>(stream), rb, hl,
+        PK_TRY(tune_shape(h, queries, nq, std::min(k, ef), ef, expand, 2, static_cast<cudaStream_t>(stream), rb, hl,
                           wp, ms));
         h->cls_rb[c] = rb;
         h->cls_hlog2[c] = hl;
