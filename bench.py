@@ -86,7 +86,7 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=2000, help="queries in the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--verbose", action="store_true")
-    p.add_argument("--paths", default="exact,f16", help="search paths to measure (exact, f16, fp8)")
+    p.add_argument("--paths", default="exact,f16,fp8", help="search paths to measure (exact, f16, fp8)")
     p.add_argument("--expand", type=int, default=1, help="entries expanded per step on the fast paths")
     p.add_argument("--fast-shape", default="", help="rows,filter_log2,warps for the fast walk instead of tuning")
     p.add_argument("--launch-check", action="store_true",

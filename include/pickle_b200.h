@@ -181,9 +181,27 @@ int pk_index_set_fast_params(pk_index *h, int32_t rows_per_batch, int32_t filter
  * 1..20 gives every width 2^log2_sets sets of 16 bytes.  The tables are
  * allocated with the search's other buffers (their size grows with the warps
  * of a launch, not with the batch); when that allocation fails the walk runs
- * without them.  The results do not depend on this setting.  No counterpart
- * in the reference. */
+ * without them.  The autotuners (pk_index_tune_fast[_classes]) also time each
+ * width without the tables and turn them off for a width where that is
+ * faster; this call clears those choices.  The results do not depend on this
+ * setting.  No counterpart in the reference. */
 int pk_index_set_fast_visited(pk_index *h, int32_t log2_sets);
+
+/* Layer-0 searches of batched insertion (pk_index_build / pk_index_add with
+ * max_batch != 1), opt-in: with min_batch > 0 the nodes of every batch of at
+ * least min_batch nodes take their ef_construction candidates at layer 0 from
+ * the FP16 walk of pk_index_search_fast (run with the batch's own rows as
+ * queries against the graph as it stood before the batch), whose exact
+ * distances then feed SelectHeuristic as the exact search's result set
+ * would; smaller batches, and every batch when max_batch == 1, use the exact
+ * search that replays the reference's heaps.  The build makes the FP16
+ * traversal copy it needs (as pk_index_prepare_fast(h, PK_TRAVERSAL_F16)
+ * would) unless an FP8 copy is prepared, in which case it keeps the exact
+ * search.  0 = off (the default).  On 10M x 128 FP16 rows (M=32, efC=200)
+ * with min_batch = 256 the build took 53.0 s instead of 62.7 s, and the
+ * graph's recall@10 at ef 64-96 was 0.005 lower.  No counterpart in the
+ * reference. */
+int pk_index_set_build_walk(pk_index *h, int64_t min_batch);
 
 /* Insertion into the walk's result list: a list of 6 or more slots of 32
  * entries per lane (ef > 160) takes the winners of a 32-candidate chunk (the

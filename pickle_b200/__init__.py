@@ -73,6 +73,7 @@ def lib() -> ctypes.CDLL:
         L.pk_index_set_fast_timing.argtypes = [P, ctypes.c_int]
         L.pk_index_set_fast_visited.argtypes = [P, I32]
         L.pk_index_set_fast_merge.argtypes = [P, I32]
+        L.pk_index_set_build_walk.argtypes = [P, I64]
         L.pk_index_fast_timing.argtypes = [P, VP, VP]
         L.pk_index_tune_fast.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
         L.pk_index_tune_fast_classes.argtypes = [P, VP, I64, I32, I32, I32, VP, VP, VP]
@@ -320,6 +321,11 @@ class HNSWIndex:
         """The walk's second-level visited tables in L2: 0 = sized by list width (default),
         -1 = off, 1..20 = 2^log2_sets sets of eight tags per warp.  Results do not depend on it."""
         _check(lib().pk_index_set_fast_visited(self._h, int(log2_sets)))
+
+    def set_build_walk(self, min_batch: int = 0) -> None:
+        """Insertion batches of at least min_batch nodes take their layer-0 candidates from the FP16
+        walk (0 = never, the default: the exact search for every batch)."""
+        _check(lib().pk_index_set_build_walk(self._h, int(min_batch)))
 
     def set_fast_merge(self, min_winners: int = 0) -> None:
         """Wide lists merge a chunk's winners at once from min_winners of them (0 = by list width,

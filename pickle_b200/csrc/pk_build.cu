@@ -11,7 +11,10 @@
 // Here a batch of nodes is inserted in three kernels:
 //   1. insert_search_kernel  one warp per new node: the descent, the per-layer
 //      searches and SelectHeuristic, all against the graph as it stood before
-//      the batch (the searches reuse the exact query path of pk_warp.cuh);
+//      the batch (the searches reuse the exact query path of pk_warp.cuh; for
+//      large batches layer 0 may instead take the candidates that the
+//      low-precision walk of pk_fast.cu found for the batch's nodes, with
+//      their exact distances recomputed here);
 //   2. add_node_kernel       one warp per (node, layer): the node's own lists;
 //   3. add_edge_kernel       one warp per (layer, target node): the reverse
 //      edges into that target, applied in batch order with AddEdge's
@@ -175,9 +178,41 @@ __global__ void __launch_bounds__(128, 4) insert_search_kernel(const DevGraph *_
                 const DevLayer Ly = gp->L[level];
                 const int32_t e0 = have_enter ? enter : Ly.ent;
                 const int top_k = level == 0 ? a.top_k0 : a.top_k0 / 2;
-                int wl = search_layer<DT, KMAX, false>(vv, lc, qr, ip, Ly, level == 0, e0, a.efc, ws, cnt, full,
-                                                       lane);
-                if (full) break;
+                int wl = 0;
+                if (level == 0 && a.l0_cand) {
+                    // the walk's candidates with their exact distances, kept
+                    // as the result heap of efc entries the search would leave
+                    const int32_t *cl = a.l0_cand + (int64_t)bi * a.l0_stride;
+                    MaxHeap W{ws.wbuf, 0};
+                    for (int j0 = 0; j0 < a.efc; j0 += 32) {
+                        const int j = j0 + lane;
+                        const int32_t v = j < a.efc ? cl[j] : -1;
+                        const bool ok = v >= 0 && v < a.pos0;
+                        const unsigned m = __ballot_sync(kFull, ok);
+                        if (ok) {
+                            const int p = __popc(m & ((1u << lane) - 1));
+                            ws.st->id[p] = v;
+                            ws.st->row[p] = v;
+                        }
+                        __syncwarp();
+                        const int nn = __popc(m);
+                        dist_rows<DT, KMAX, false>(vv, lc, qr, ip, ws.st->row, ws.st->d, nn, lane);
+                        __syncwarp();
+                        if (lane == 0)
+                            for (int t = 0; t < nn; t++) {
+                                const float d = ws.st->d[t];
+                                if (W.len < a.efc || W.a[0].d > d) {
+                                    W.push(Ent{d, ws.st->id[t]});
+                                    if (W.len > a.efc) W.pop();
+                                }
+                            }
+                        __syncwarp();
+                    }
+                    wl = __shfl_sync(kFull, W.len, 0);
+                } else {
+                    wl = search_layer<DT, KMAX, false>(vv, lc, qr, ip, Ly, level == 0, e0, a.efc, ws, cnt, full, lane);
+                    if (full) break;
+                }
                 // The batch's earlier nodes (j < bi) are not in the graph yet;
                 // offer every one that joins this layer to the result set, as
                 // if the search had reached it.  With one node per batch there

@@ -26,6 +26,11 @@ struct InsertSearchArgs {
     int32_t *work;            // [0] node counter, [1] scratch overflows
     WarpGlobalScratch gs;
     int32_t wcap;
+    // layer 0 from a walk's candidate lists instead of the exact search:
+    // node i's efc best traversal candidates at l0_cand[i * l0_stride]
+    // (layer-0 ids, -1 = none); null = the exact search
+    const int32_t *l0_cand;
+    int32_t l0_stride;
 };
 
 // Kernel 2: AddNode for each (node, layer <= its level).  With meta_only it

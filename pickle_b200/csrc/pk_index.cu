@@ -208,9 +208,15 @@ struct pk_index {
     // the walk's visited tables in L2: 0 = sized by list width, -1 = off,
     // > 0 = log2 of the sets for every width
     int fast_vt = 0;
+    // per list-width class: -1 = the tuner found the width faster without
+    // the L2 tables (0 = as fast_vt)
+    int cls_vt[pk::kSlotClasses] = {};
     // winners of a 32-candidate chunk from which the walk merges them into a
     // wide list at once: 0 = by list width, -1 = never (one by one)
     int fast_merge = 0;
+    // insertion batches of at least this many nodes take their layer-0
+    // candidates from the FP16 walk (0 = none: the exact search throughout)
+    int64_t build_walk = 0;
 
     size_t dev_bytes = 0;
 
@@ -534,6 +540,13 @@ void free_batch(pk_index *h, BatchBufs &b) {
     b = BatchBufs{};
 }
 
+int build_traversal(pk_index *h, int trav);
+int refresh_traversal(pk_index *h);
+int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_queries, int64_t nq, int32_t k,
+                    int32_t ef, const int32_t *k_arr, const int32_t *ef_arr, int32_t stride, int32_t *ids,
+                    float *dists, int32_t *counters, int32_t expand, cudaStream_t s, bool walk_only = false);
+int fast_status(pk_index *h, FastCtx &c, cudaStream_t s);
+
 // Inserts count rows, row i taken from rows + i*dim*esz with external id
 // ext[i], in that order.
 int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t count, int32_t max_batch) {
@@ -633,6 +646,10 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
     PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, bm_words, vl_cap, tail));
 
     const int capmax = (int)top_k0;
+    // layer-0 candidates from the FP16 walk for large batches (an FP8 copy,
+    // or one-node batches, keep the exact search)
+    const int64_t walk_min = h->build_walk > 0 ? h->build_walk : INT64_MAX;
+    const bool walk_ok = max_batch != 1 && h->efc <= pk::kFastMaxEf && (h->trav == 0 || h->trav == pk::kTravF16);
     std::vector<int32_t> node_id, item_node, item_level, item_id, item_down, top_ins, bext;
     int64_t done = 0, bsize = 1;
     while (done < count) {
@@ -686,6 +703,14 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
         na.counts = bb.counts;
         na.meta_only = 1;
         PK_CUDA(pk::launch_add_node(h->dg, na, s));
+        // 0. for a large batch on a graph of some size, the walk's layer-0
+        // candidate lists for the batch's nodes (their rows are the queries)
+        const bool use_walk = walk_ok && nonempty && nb >= walk_min && h->n0() >= 4 * h->efc;
+        if (use_walk) {
+            if (h->trav == 0) PK_TRY(build_traversal(h, pk::kTravF16));
+            PK_TRY(run_search_fast(h, h->fctx, h->hg.vec0 + (n0_before + done) * h->row_bytes, false, nb, 1,
+                                   (int32_t)h->efc, nullptr, nullptr, 1, nullptr, nullptr, nullptr, 1, s, true));
+        }
         // 1. searches + SelectHeuristic (retried with more scratch on overflow)
         for (int attempt = 0;; attempt++) {
             PK_CUDA(cudaMemsetAsync(h->bs.work, 0, sizeof(int32_t) * 2, s));
@@ -704,6 +729,8 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
             a.work = h->bs.work;
             a.gs = h->bs.view();
             a.wcap = wcap;
+            a.l0_cand = use_walk ? h->fctx.d_cand : nullptr;
+            a.l0_stride = 32 * pk::list_slots((int)std::min<int64_t>(h->efc, pk::kFastMaxEf));
             const int64_t grid = std::min<int64_t>((nb + wpb - 1) / wpb, max_grid);
             PK_CUDA(pk::launch_insert_search(h->dg, h->dtype, h->lc, a, (int)grid, wpb, smem, s));
             int32_t over = 0;
@@ -711,10 +738,13 @@ int insert_rows(pk_index *h, const uint8_t *rows, const int32_t *ext, int64_t co
             PK_CUDA(cudaStreamSynchronize(s));
             if (over == 0) break;
             if (attempt >= 3 || tail >= (1LL << 24)) return fail(PK_ERR_OVERFLOW, "insertion search outgrew scratch");
+            // (the walk's candidates stay valid for the retry)
             tail *= 4;
             PK_TRY(ensure_scratch(h, h->bs, max_grid * wpb, bm_words, vl_cap, tail));
             PK_CUDA(cudaMemsetAsync(bb.counts, 0, 4 * nb * max_levels, s));
         }
+        // a walk whose row fetch timed out left incomplete lists
+        if (use_walk) PK_TRY(fast_status(h, h->fctx, s));
         // 2. AddNode for every (node, layer)
         na.meta_only = 0;
         PK_CUDA(pk::launch_add_node(h->dg, na, s));
@@ -901,7 +931,7 @@ int walk_plan(pk_index *h, int64_t nq, int slots, bool binned, int expand, ClsPl
         const int nb = pk::walk_blocks_per_sm(h->trav, sl, expand, P.ws.wpb, P.ws.smem);
         if (nb <= 0) return fail(PK_ERR_CUDA, "walk kernel cannot be resident");
         P.grid = std::min<int64_t>((int64_t)nb * h->num_sms, (nq + P.ws.wpb - 1) / P.ws.wpb);
-        if (h->fast_vt >= 0) {
+        if (h->fast_vt >= 0 && h->cls_vt[cls] >= 0) {
             int l = h->fast_vt > 0 ? h->fast_vt : pk::visited_log2sets(sl, ids0);
             l = std::max(l, pk::idbits_for(ids0) - 15);
             P.vt_log2 = l;
@@ -914,9 +944,12 @@ int walk_plan(pk_index *h, int64_t nq, int slots, bool binned, int expand, ClsPl
 
 // Low-precision walk, then exact re-rank of each query's final list.  Fully
 // asynchronous on stream s.
+// walk_only: the queries are padded device rows (row_bytes apart), and the
+// call ends after the walk, leaving each query's candidate list in c.d_cand
+// (no re-rank; k, k_arr, stride, ids and dists are unused).
 int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_queries, int64_t nq, int32_t k,
                     int32_t ef, const int32_t *k_arr, const int32_t *ef_arr, int32_t stride, int32_t *ids,
-                    float *dists, int32_t *counters, int32_t expand, cudaStream_t s) {
+                    float *dists, int32_t *counters, int32_t expand, cudaStream_t s, bool walk_only) {
     if (h->trav == 0) return fail(PK_ERR_STATE, "pk_index_prepare_fast has not been called");
     if (ef > pk::kFastMaxEf) return fail(PK_ERR_ARG, "ef too large for the fast path (max 1024)");
     PK_TRY(refresh_traversal(h));
@@ -933,7 +966,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
     // exact queries (padded rows) and traversal queries
     const size_t w = (size_t)(h->dim * h->esz);
     const uint8_t *qx = static_cast<const uint8_t *>(queries);
-    if (host_queries || w != (size_t)h->row_bytes || ((uintptr_t)queries & 15) != 0) {
+    if (!walk_only && (host_queries || w != (size_t)h->row_bytes || ((uintptr_t)queries & 15) != 0)) {
         PK_TRY(ensure_buf(h, &c.d_fq, c.fq_n, nq * h->row_bytes));
         if (w != (size_t)h->row_bytes) PK_CUDA(cudaMemsetAsync(c.d_fq, 0, (size_t)(nq * h->row_bytes), s));
         PK_CUDA(cudaMemcpy2DAsync(c.d_fq, (size_t)h->row_bytes, queries, w, w, (size_t)nq,
@@ -1021,6 +1054,7 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
         }
     }
     if (timed) PK_CUDA(cudaEventRecord(c.ev[1], s));
+    if (walk_only) return PK_OK;
 
     int rwpb = 4;
     size_t rsmem = (size_t)rwpb * pk::rerank_layout(cs, h->row_bytes).total;
@@ -1533,11 +1567,13 @@ static int pk_index_prepare_fast_impl(pk_index *h, int traversal) {
 // was.  reps = timed runs per shape (after one warm-up run); a shape's time is
 // the fastest of them (the least disturbed by whatever else shares the GPU).
 int tune_shape(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef, int32_t expand, int reps,
-               cudaStream_t s, int &brb, int &bh, int &bw, float &best) {
+               cudaStream_t s, int &brb, int &bh, int &bw, float &best, int &bvt) {
     PK_TRY(ensure_buf(h, &h->d_fids, h->fids_n, nq * k));
     PK_TRY(ensure_buf(h, &h->d_fdists, h->fdists_n, nq * k));
     const int cls = pk::slot_class(ef);
     const int keep_rb = h->cls_rb[cls], keep_h = h->cls_hlog2[cls], keep_w = h->cls_wpb[cls];
+    const int keep_vt = h->cls_vt[cls];
+    bvt = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     PK_CUDA(cudaEventCreate(&e0));
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -1586,6 +1622,7 @@ int tune_shape(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t 
     // (with the visited tables in L2 behind it, small shared-memory tables
     // that leave room for more warps are often the fastest)
     const int hls[] = {6, 8, 9, 10, 11, 12, 13};
+    h->cls_vt[cls] = 0;
     const int wps[] = {1, 2, 4};
     const int rbs1[] = {16, 32};
     for (int rb : rbs1)
@@ -1596,6 +1633,16 @@ int tune_shape(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t 
     const int rbs[] = {8, 16, 24, 32, 48, 64};
     for (int rb : rbs)
         if (rc == PK_OK && best >= 0.f && rb != r1) time_shape(rb, h1, w1);
+    // stage 3: the best shape without the visited tables in L2 (narrow lists
+    // meet few nodes again, and the tables' round trip can cost more than
+    // the rows they spare)
+    if (rc == PK_OK && best >= 0.f && h->fast_vt >= 0) {
+        const float with = best;
+        h->cls_vt[cls] = -1;
+        time_shape(brb, bh, bw);
+        if (best < with) bvt = -1;
+    }
+    h->cls_vt[cls] = keep_vt;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     h->cls_rb[cls] = keep_rb;
@@ -1620,13 +1667,16 @@ static int tune_check(pk_index *h, const void *queries, int64_t nq, int32_t k, i
 static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq, int32_t k, int32_t ef,
                                    int32_t expand, int32_t *out_shape, float *out_ms, void *stream) {
     PK_TRY(tune_check(h, queries, nq, k, ef));
-    int rb = 0, hl = 0, wp = 0;
+    int rb = 0, hl = 0, wp = 0, vt = 0;
     float ms = 0.f;
-    PK_TRY(tune_shape(h, queries, nq, k, ef, expand, 2, static_cast<cudaStream_t>(stream), rb, hl, wp, ms));
+    PK_TRY(tune_shape(h, queries, nq, k, ef, expand, 2, static_cast<cudaStream_t>(stream), rb, hl, wp, ms, vt));
     h->fast_rb = rb;
     h->fast_hlog2 = hl;
     h->fast_wpb = wp;
-    for (int c = 0; c < pk::kSlotClasses; c++) h->cls_rb[c] = h->cls_hlog2[c] = h->cls_wpb[c] = 0;
+    for (int c = 0; c < pk::kSlotClasses; c++) {
+        h->cls_rb[c] = h->cls_hlog2[c] = h->cls_wpb[c] = 0;
+        h->cls_vt[c] = vt;
+    }
     if (out_shape) {
         out_shape[0] = rb;
         out_shape[1] = hl;
@@ -1648,10 +1698,11 @@ static int pk_index_tune_fast_classes_impl(pk_index *h, const void *queries, int
         const int lo = c == 0 ? 1 : 32 * pk::slot_class_width(c - 1) + 1;
         if (lo > max_ef) continue;
         const int ef = std::min(32 * pk::slot_class_width(c), std::min(max_ef, pk::kFastMaxEf));
-        int rb = 0, hl = 0, wp = 0;
+        int rb = 0, hl = 0, wp = 0, vt = 0;
         float ms = 0.f;
         PK_TRY(tune_shape(h, queries, nq, std::min(k, ef), ef, expand, 2, static_cast<cudaStream_t>(stream), rb, hl,
-                          wp, ms));
+                          wp, ms, vt));
+        h->cls_vt[c] = vt;
         h->cls_rb[c] = rb;
         h->cls_hlog2[c] = hl;
         h->cls_wpb[c] = wp;
@@ -2501,6 +2552,14 @@ int pk_index_set_fast_visited(pk_index *h, int32_t log2_sets) {
     if (!h) return fail(PK_ERR_ARG, "NULL handle");
     if (log2_sets < -1 || log2_sets > 20) return fail(PK_ERR_ARG, "log2_sets must be -1, 0 or 1..20");
     h->fast_vt = log2_sets;
+    for (int c = 0; c < pk::kSlotClasses; c++) h->cls_vt[c] = 0;  // the tuners' per-width choices
+    return PK_OK;
+}
+
+int pk_index_set_build_walk(pk_index *h, int64_t min_batch) {
+    if (!h) return fail(PK_ERR_ARG, "NULL handle");
+    if (min_batch < 0) return fail(PK_ERR_ARG, "min_batch must be 0 (off) or positive");
+    h->build_walk = min_batch;
     return PK_OK;
 }
 

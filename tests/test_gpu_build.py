@@ -111,3 +111,24 @@ def test_batched_build_reaches_reference_recall(name, gpu, ref_bin, tmp_path):
     for ef in efs:
         tol = build_recall_tolerance(r_ref[ef], r_dev[ef], 10 * len(queries))
         assert np.mean(r_dev[ef]) >= np.mean(r_ref[ef]) - tol, (ef, r_dev[ef], r_ref[ef], tol)
+
+
+@pytest.mark.parametrize("min_batch", [256, 1])
+def test_walk_assisted_build_keeps_recall(min_batch, gpu):
+    """Insertion batches that take their layer-0 candidates from the FP16 walk
+    (batches of 256 nodes or more, or every batch with min_batch = 1) build a
+    graph nearly as good as the exact-search build of the same rows and
+    levels: recall@10 at equal ef within 0.01."""
+    base, queries = datasets.gmm_f16(20000, 300, 64, ncomp=32, sigma=0.5, seed=21)
+    gt, _ = datasets.exact_knn(base, queries, 10, "l2")
+    rec = {}
+    for mode in (min_batch, 0):
+        idx = HNSWIndex(64, np.float16, "l2", M=16, ef_construction=100)
+        idx.set_seed(21)
+        idx.set_build_walk(mode)
+        idx.build(base)
+        rec[mode] = {ef: datasets.recall_at_k(idx.search(queries, 10, ef)[0], gt, 10) for ef in (16, 32, 64)}
+        idx.close()
+    for ef in (16, 32, 64):
+        assert rec[min_batch][ef] >= rec[0][ef] - 0.01, (ef, rec)
+    assert rec[min_batch][64] >= 0.95, rec
