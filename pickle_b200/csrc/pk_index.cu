@@ -1673,9 +1673,11 @@ static int pk_index_tune_fast_impl(pk_index *h, const void *queries, int64_t nq,
     h->fast_rb = rb;
     h->fast_hlog2 = hl;
     h->fast_wpb = wp;
+    // the tables' choice holds for the tuned ef's width only (wider lists
+    // meet many more nodes again)
     for (int c = 0; c < pk::kSlotClasses; c++) {
         h->cls_rb[c] = h->cls_hlog2[c] = h->cls_wpb[c] = 0;
-        h->cls_vt[c] = vt;
+        h->cls_vt[c] = c == pk::slot_class(ef) ? vt : 0;
     }
     if (out_shape) {
         out_shape[0] = rb;
