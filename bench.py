@@ -276,9 +276,12 @@ def profiled_traffic(workload_key, path):
     try:
         with open(os.path.join(ROOT, "profiles", f"walk_kernel_{workload_key}_traffic.json")) as f:
             d = json.load(f)
-        return d if d.get("path") == path else None
     except (OSError, ValueError):
         return None
+    if "paths" in d:
+        p = d["paths"].get(path)
+        return dict(p, source=d.get("source")) if p else None
+    return d if d.get("path") == path else None
 
 
 def cpu_reference(graph_path, queries, k, ef, kq, efq, repeat, warmup=0):
