@@ -78,7 +78,8 @@ struct TravView {
 // ------------------------------------------------------ asynchronous rows --
 // Rows move from global to shared memory with one bulk copy per row, issued
 // by as many lanes as there are rows and completing on a per-warp mbarrier
-// that counts the bytes.  A warp waits once per batch of rows.
+// that counts the bytes, with an L2 evict-first hint.  A warp waits once per
+// batch of rows.
 
 // Bound on the wait for one batch of rows: 2 s of the global timer (a batch
 // lands in microseconds), checked every 64 polls.
@@ -128,12 +129,16 @@ __device__ __forceinline__ bool fetch_rows(RowFetch &f, const TravView &tv, cons
                      "r"((uint32_t)(n * tv.row_bytes))
                      : "memory");
     __syncwarp();
+    // rows are read once per visit: marked first to leave L2, so that the
+    // walks' visited tables (and the hot adjacency rows) stay there longer
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
     for (int t = lane; t < n; t += 32) {
         const int32_t r = rows[t];
         asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                smem_u32(f.buf + t * f.stride)),
-            "l"(tv.row(r)), "r"((uint32_t)tv.row_bytes), "r"(smem_u32(f.bar))
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+            "%4;" ::"r"(smem_u32(f.buf + t * f.stride)),
+            "l"(tv.row(r)), "r"((uint32_t)tv.row_bytes), "r"(smem_u32(f.bar)), "l"(pol)
             : "memory");
     }
     bool ok = mbar_poll(f.bar, f.parity);
