@@ -217,8 +217,11 @@ int pk_index_set_fast_merge(pk_index *h, int32_t min_winners);
  * pk_index_search_fast_host call on the handle records CUDA events on its
  * stream around the walk kernel and the re-rank kernel;
  * pk_index_fast_timing waits for the last call's events and returns the two
- * device durations in milliseconds.  Off by default (serving slots never
- * record).  No counterpart in the reference. */
+ * device durations in milliseconds.  With per-query ef each list width's
+ * re-rank follows its walk on that width's stream: the walk time is then the
+ * span until the last width's walk ends (the earlier widths' re-ranks run
+ * inside it), the re-rank time what follows it.  Off by default (serving
+ * slots never record).  No counterpart in the reference. */
 int pk_index_set_fast_timing(pk_index *h, int enable);
 int pk_index_fast_timing(pk_index *h, float *walk_ms, float *rerank_ms);
 

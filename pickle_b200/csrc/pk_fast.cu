@@ -961,7 +961,8 @@ __global__ void __launch_bounds__(128)
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
-    const RerankLayout lay = rerank_layout(a.cand_stride, a.row_bytes);
+    const int cap = a.cand_cap > 0 ? a.cand_cap : a.cand_stride;
+    const RerankLayout lay = rerank_layout(cap, a.row_bytes);
     unsigned char *my = smem + (size_t)wib * lay.total;
     Stage *st = reinterpret_cast<Stage *>(my);
     float *sd = reinterpret_cast<float *>(my + lay.sd);
@@ -970,9 +971,11 @@ __global__ void __launch_bounds__(128)
     const VecView vv{gp->vec0, gp->zero_row, gp->row_bytes};
     const bool ip = gp->metric == PK_METRIC_IP;
     const bool walk_failed = *a.status != 0;
-    for (int64_t q = (int64_t)blockIdx.x * wpb + wib; q < a.nq; q += (int64_t)gridDim.x * wpb) {
+    const int64_t nlim = a.qcount ? (int64_t)*a.qcount : a.nq;
+    for (int64_t i = (int64_t)blockIdx.x * wpb + wib; i < nlim; i += (int64_t)gridDim.x * wpb) {
+        const int64_t q = a.qlist ? a.qlist[i] : i;
         const int k = max(0, min(a.k_arr ? a.k_arr[q] : a.k, a.out_stride));
-        const int L = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, a.cand_stride));
+        const int L = max(1, min(a.ef_arr ? a.ef_arr[q] : a.ef, cap));
         int32_t *oid = a.out_ids + q * a.out_stride;
         float *od = a.out_dists + q * a.out_stride;
         if (walk_failed) {

@@ -139,7 +139,8 @@ struct RerankArgs {
     int32_t k, ef;              // uniform values (ef also bounds ef_arr)
     const int32_t *k_arr, *ef_arr;
     int32_t out_stride;
-    int32_t cand_stride;
+    int32_t cand_stride;        // ints between two queries' lists in cand
+    int32_t cand_cap;           // entries a list may hold (<= cand_stride; 0 = cand_stride): bounds ef, sizes the sort
     int32_t *out_ids;
     float *out_dists;
     const int32_t *ext0;
@@ -147,6 +148,8 @@ struct RerankArgs {
     const int32_t *status;      // the walk's status: nonzero = its lists are incomplete
     const uint8_t *queries;     // exact queries, padded rows of row_bytes
     int64_t row_bytes;
+    const int32_t *qlist;       // the queries to re-rank (null: 0 .. nq-1)
+    const int32_t *qcount;      // device count of qlist's entries (null: nq)
 };
 
 __host__ __device__ inline int pow2_at_least(int x) {

@@ -136,6 +136,10 @@ struct FastCtx {
     // first use)
     cudaStream_t aux[pk::kSlotClasses] = {};
     cudaEvent_t fork = nullptr, join[pk::kSlotClasses] = {};
+    // timed per-width launches: the end of each width's walk (its re-rank
+    // follows on the same stream), for the widths in wend_mask
+    cudaEvent_t wend[pk::kSlotClasses] = {};
+    uint32_t wend_mask = 0;
 };
 
 // Releases a context's streams and events (not its buffers).
@@ -143,6 +147,8 @@ void release_ctx_sync(FastCtx &c) {
     for (cudaEvent_t &e : c.ev)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t &e : c.join)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t &e : c.wend)
         if (e) cudaEventDestroy(e);
     if (c.fork) cudaEventDestroy(c.fork);
     for (cudaStream_t &t : c.aux)
@@ -1013,15 +1019,52 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
         for (cudaEvent_t &e : c.ev)
             if (!e) PK_CUDA(cudaEventCreate(&e));
         PK_CUDA(cudaEventRecord(c.ev[0], s));
+        c.wend_mask = 0;
     }
     if (binned) {
         if (!c.fork) PK_CUDA(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
         PK_CUDA(cudaEventRecord(c.fork, s));
     }
+    // the exact re-rank of the lists of cap entries (at most cand_stride) of
+    // the queries in qlist (all queries when null), on stream ls
+    auto rerank = [&](cudaStream_t ls, int cap, int32_t ef_bound, const int32_t *qlist, const int32_t *qcount,
+                      int64_t nmax) -> int {
+        int rwpb = 4;
+        size_t rsmem = (size_t)rwpb * pk::rerank_layout(cap, h->row_bytes).total;
+        while (rwpb > 1 && rsmem > 200 * 1024) {
+            rwpb /= 2;
+            rsmem = (size_t)rwpb * pk::rerank_layout(cap, h->row_bytes).total;
+        }
+        const int rnb = pk::rerank_blocks_per_sm(h->dtype, h->lc, rwpb, rsmem);
+        if (rnb <= 0) return fail(PK_ERR_CUDA, "re-rank kernel cannot be resident");
+        const int64_t rgrid = std::min<int64_t>((int64_t)rnb * h->num_sms, (nmax + rwpb - 1) / rwpb);
+        pk::RerankArgs r{};
+        r.nq = nq;
+        r.k = k;
+        r.ef = ef_bound;
+        r.k_arr = k_arr;
+        r.ef_arr = ef_arr;
+        r.out_stride = stride;
+        r.cand_stride = cs;
+        r.cand_cap = cap;
+        r.out_ids = ids;
+        r.out_dists = dists;
+        r.ext0 = h->hg.L[0].ext;
+        r.cand = c.d_cand;
+        r.status = c.d_work + kWorkStatus;
+        r.queries = qx;
+        r.row_bytes = h->row_bytes;
+        r.qlist = qlist;
+        r.qcount = qcount;
+        PK_CUDA(pk::launch_rerank(h->dg, h->dtype, h->lc, r, (int)std::max<int64_t>(rgrid, 1), rwpb, rsmem, ls));
+        return PK_OK;
+    };
     // widest first: each launch fills the GPU and the next one's blocks take
     // the SMs its warps leave as its work runs out, so the launch that ends
     // the batch - whose tail nothing fills - is the one with the shortest
-    // queries
+    // queries.  With per-query ef each width's re-rank follows its walk on
+    // the width's own stream, so it overlaps the other widths' walks instead
+    // of waiting for the last of them; its sort takes that width's lists only.
     for (int cls = pk::kSlotClasses - 1; cls >= 0; cls--) {
         const int sl = pk::slot_class_width(cls);
         if (sl > slots || (!binned && sl != slots)) continue;
@@ -1049,38 +1092,20 @@ int run_search_fast(pk_index *h, FastCtx &c, const void *queries, bool host_quer
         a.qcount = binned ? c.d_work + kWorkCounts + cls : nullptr;
         PK_CUDA(pk::launch_walk(h->dg, h->trav, sl, a, (int)P.grid, P.ws.wpb, P.ws.smem, ls));
         if (binned) {
+            if (timed) {
+                if (!c.wend[cls]) PK_CUDA(cudaEventCreate(&c.wend[cls]));
+                PK_CUDA(cudaEventRecord(c.wend[cls], ls));
+                c.wend_mask |= 1u << cls;
+            }
+            if (!walk_only)
+                PK_TRY(rerank(ls, std::min(32 * sl, cs), std::min(ef, 32 * sl), a.qlist, a.qcount, nq));
             PK_CUDA(cudaEventRecord(c.join[cls], ls));
             PK_CUDA(cudaStreamWaitEvent(s, c.join[cls], 0));
         }
     }
     if (timed) PK_CUDA(cudaEventRecord(c.ev[1], s));
     if (walk_only) return PK_OK;
-
-    int rwpb = 4;
-    size_t rsmem = (size_t)rwpb * pk::rerank_layout(cs, h->row_bytes).total;
-    while (rwpb > 1 && rsmem > 200 * 1024) {
-        rwpb /= 2;
-        rsmem = (size_t)rwpb * pk::rerank_layout(cs, h->row_bytes).total;
-    }
-    const int rnb = pk::rerank_blocks_per_sm(h->dtype, h->lc, rwpb, rsmem);
-    if (rnb <= 0) return fail(PK_ERR_CUDA, "re-rank kernel cannot be resident");
-    const int64_t rgrid = std::min<int64_t>((int64_t)rnb * h->num_sms, (nq + rwpb - 1) / rwpb);
-    pk::RerankArgs r{};
-    r.nq = nq;
-    r.k = k;
-    r.ef = ef;
-    r.k_arr = k_arr;
-    r.ef_arr = ef_arr;
-    r.out_stride = stride;
-    r.cand_stride = cs;
-    r.out_ids = ids;
-    r.out_dists = dists;
-    r.ext0 = h->hg.L[0].ext;
-    r.cand = c.d_cand;
-    r.status = c.d_work + kWorkStatus;
-    r.queries = qx;
-    r.row_bytes = h->row_bytes;
-    PK_CUDA(pk::launch_rerank(h->dg, h->dtype, h->lc, r, (int)rgrid, rwpb, rsmem, s));
+    if (!binned) PK_TRY(rerank(s, cs, ef, nullptr, nullptr, nq));
     if (timed) PK_CUDA(cudaEventRecord(c.ev[2], s));
     return PK_OK;
 }
@@ -2583,8 +2608,24 @@ int pk_index_fast_timing(pk_index *h, float *walk_ms, float *rerank_ms) {
     const FastCtx &c = h->fctx;
     if (!h->fast_timing || !c.ev[2]) return fail(PK_ERR_STATE, "no timed fast search has run");
     PK_CUDA(cudaEventSynchronize(c.ev[2]));
-    PK_CUDA(cudaEventElapsedTime(walk_ms, c.ev[0], c.ev[1]));
-    PK_CUDA(cudaEventElapsedTime(rerank_ms, c.ev[1], c.ev[2]));
+    if (c.wend_mask == 0) {
+        PK_CUDA(cudaEventElapsedTime(walk_ms, c.ev[0], c.ev[1]));
+        PK_CUDA(cudaEventElapsedTime(rerank_ms, c.ev[1], c.ev[2]));
+        return PK_OK;
+    }
+    // per-width launches: the walks span from the start to the end of the
+    // last width's walk; the re-ranks of the widths that ended earlier ran
+    // inside that span, and what follows it is the last re-ranks' time
+    float walk = 0.f, all = 0.f;
+    for (int cls = 0; cls < pk::kSlotClasses; cls++) {
+        if (!((c.wend_mask >> cls) & 1u)) continue;
+        float t = 0.f;
+        PK_CUDA(cudaEventElapsedTime(&t, c.ev[0], c.wend[cls]));
+        walk = std::max(walk, t);
+    }
+    PK_CUDA(cudaEventElapsedTime(&all, c.ev[0], c.ev[2]));
+    *walk_ms = walk;
+    *rerank_ms = std::max(0.f, all - walk);
     return PK_OK;
 }
 
