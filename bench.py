@@ -280,7 +280,7 @@ def profiled_traffic(workload_key, path):
         return None
     if "paths" in d:
         p = d["paths"].get(path)
-        return dict(p, source=d.get("source")) if p else None
+        return dict(p, source=p.get("source", d.get("source"))) if p else None
     return d if d.get("path") == path else None
 
 

@@ -5,7 +5,9 @@
 // also what bounds it.  These kernels answer the same question - the k
 // nearest neighbours found by a best-first walk of the HNSW graph with a
 // result set of ef entries (include/hnsw.hpp:373-444) - with data structures
-// suited to a warp, and are judged by recall.  Two launches per batch:
+// suited to a warp, and are judged by recall.  Two kernels, a walk then a
+// re-rank (with per-query ef: one of each per list width, on that width's
+// own stream):
 //
 // walk_kernel (one query per warp, work stealing, per-query ef):
 //   * traversal distances come from a low-precision copy of the vectors,
@@ -35,9 +37,9 @@
 //   depend on the tables' sizes (or on whether the L2 table is used at all)
 //   or on the batch order.
 //
-// rerank_kernel (one query per warp): exact distances from the original
-// vectors for the ef listed ids, sorted by (distance, id); the k best are
-// written with their external ids.
+// rerank_kernel (one query per warp; all queries, or one list width's):
+// exact distances from the original vectors for the ef listed ids, sorted by
+// (distance, id); the k best are written with their external ids.
 //
 // There is no host round trip, so a batch can be captured in a CUDA graph.
 #include <cuda_fp16.h>
