@@ -454,16 +454,19 @@ struct RegList {
     }
 
     // The first position of an empty list of L: the entry point (not yet
-    // expanded).
+    // expanded).  The slot is chosen at run time, so every slot is written
+    // through a mask: a branch on (s == slot) lets the compiler fold the
+    // unrolled writes back into one store at a run-time index, which moves
+    // the whole list out of registers into local memory.
     __device__ __forceinline__ void put_first(int L, uint32_t nk, uint32_t nid, int lane) {
         const int p0 = 32 * S - L;
         if (lane == p0 / S) {
 #pragma unroll
-            for (int s = 0; s < S; s++)
-                if (s == p0 % S) {
-                    k[s] = nk;
-                    id[s] = nid;
-                }
+            for (int s = 0; s < S; s++) {
+                const uint32_t m = 0u - (uint32_t)(s == p0 % S);
+                k[s] ^= (k[s] ^ nk) & m;
+                id[s] ^= (id[s] ^ nid) & m;
+            }
             xm &= ~(1u << (p0 % S));
         }
     }
@@ -615,9 +618,9 @@ struct RegList {
         int32_t v = 0;
         if (lane == fl) {
             const int fs = __ffs(un) - 1;
+            // masked, like put_first: no read at a run-time index
 #pragma unroll
-            for (int s = 0; s < S; s++)
-                if (s == fs) v = (int32_t)id[s];
+            for (int s = 0; s < S; s++) v |= (int32_t)(id[s] & (0u - (uint32_t)(s == fs)));
             xm |= 1u << fs;
         }
         return __shfl_sync(kFull, v, fl);
