@@ -41,12 +41,18 @@ def _compile(src: str, force: bool) -> str:
     if not force and os.path.exists(obj):
         if os.path.getmtime(obj) >= max(os.path.getmtime(src), _headers_mtime()):
             return obj
-    cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
+    # ptxas's report (registers, stack frame and spills of every kernel) is
+    # kept beside the object: tests read it to check that the walk's list
+    # stays in registers
+    cmd = [NVCC] + ARCH + FLAGS + ["-Xptxas", "-v", "-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [NVCC] + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{p.stderr}")
+    if src.endswith(".cu"):
+        with open(obj + ".ptxas.txt", "w") as f:
+            f.write(p.stderr)
     return obj
 
 
